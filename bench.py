@@ -1,0 +1,440 @@
+#!/usr/bin/env python
+"""Headline benchmark: entropy-coded int8 matvec on B200.
+
+Metric: int8-equivalent GB/s ((rows*cols + B*cols + 4*B*rows) bytes per matvec
+/ time) and us per matvec, with bit-exact int32 output, against the dense int8
+dp4a matvec on the same GPU.
+
+Workload (one step): the single-vector 7B-layer shapes W_q 4096x4096,
+11008x4096 and 4096x11008, each at sigma 4 and sigma 2
+(clamp(round(N(0, sigma^2)))), each encoded once with one global table and once
+with per-row tables, in this library's Q8-stripe layout: 12 matvecs with one
+int8 x each (B = 1).  All 12 compressed matrices together are ~200 MB, larger
+than the 126 MB L2, and each is read once per step, so every read comes from
+HBM.  Inputs are synthetic and seeded; there is no public dataset.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's CPU implementation of the path (the
+oracle's C restatement of the ans-warp-rows decoder, buffered/
+ans-warp-rows-kernel.cu, with all host threads) on the same shapes.
+"""
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPES = [(4096, 4096), (11008, 4096), (4096, 11008)]
+SIGMAS = [4.0, 2.0]
+METRIC = "us/matvec & int8-equiv GB/s vs dense dp4a int8 on B200, bit-exact int32 output"
+UNIT = "GB/s"
+L2_BYTES = 126 * 2 ** 20
+
+
+def gen_matrix(shape, sigma, seed):
+    rng = np.random.default_rng(seed)
+    out = np.empty(shape, np.int8)
+    step = max(1, (1 << 24) // shape[1])
+    for r0 in range(0, shape[0], step):
+        z = rng.standard_normal((min(step, shape[0] - r0), shape[1]), dtype=np.float32) * np.float32(sigma)
+        out[r0:r0 + z.shape[0]] = np.clip(np.rint(z), -127, 127).astype(np.int8)
+    return out
+
+
+def workload(seed=20251203):
+    mats = []
+    for i, shape in enumerate(SHAPES):
+        for j, s in enumerate(SIGMAS):
+            mats.append(dict(shape=shape, sigma=s, W=gen_matrix(shape, s, seed + 10 * i + j)))
+    return mats
+
+
+def int8_equiv_bytes(rows, cols, B=1):
+    return rows * cols + B * cols + 4 * B * rows
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons through NVML while running."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown", 0x1: "gpu_idle"}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            self.sample()
+            time.sleep(0.005)
+
+    def sample(self):
+        if not self.nv:
+            return
+        try:
+            self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            for bit, name in self.REASONS.items():
+                if r & bit and name != "gpu_idle":
+                    self.reasons.add(name)
+        except Exception:
+            pass
+
+    def __enter__(self):
+        self.sample()
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self.t.join()
+        self.sample()
+
+    def summary(self):
+        return {"sm_mhz": float(np.median(self.samples)) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------ CPU legs
+
+def cpu_reference_pass(awr_mats, x_by_cols, nthreads):
+    """One pass of the oracle's AWR decode + matvec over the AWR-encoded matrices."""
+    import oracle
+    nbytes = 0
+    for m in awr_mats:
+        rows, cols = m["shape"]
+        y = oracle.awr_matvec(m["compressed"], m["offsets"], rows, cols, m["ppf"], m["cum"], m["prob"],
+                              x_by_cols[cols], nthreads=nthreads)
+        assert y.shape == (rows,)
+        nbytes += int8_equiv_bytes(rows, cols)
+    return nbytes
+
+
+def awr_encode_all(mats):
+    from matvans_b200 import codec
+    out = []
+    for m in mats:
+        comp, offs, mn, cdf = codec.compress_ans_warp_rows(m["W"])
+        p, pc, pp = codec.decoder_model_from_128bit_encoder_model(mn, cdf)
+        out.append(dict(shape=m["shape"], sigma=m["sigma"], compressed=comp, offsets=offs,
+                        ppf=codec.pack_4bytes(p), cum=codec.pack_4bytes(pc), prob=codec.pack_4bytes(pp)))
+    return out
+
+
+def cpu_baseline(mats, x_by_cols, budget_s=8.0):
+    nthreads = os.cpu_count() or 1
+    awr = awr_encode_all(mats)
+    t0 = time.perf_counter()
+    nbytes, passes = 0, 0
+    while True:
+        nbytes += cpu_reference_pass(awr, x_by_cols, nthreads)
+        passes += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": nbytes / dt / 1e9, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{passes} pass(es) over the 6 ans-warp-rows encodings (3 shapes x sigma 4,2) of the "
+                      f"workload, oracle C decode+matvec, {nthreads} threads, {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    mats = workload()
+    rng = np.random.default_rng(7)
+    x_by_cols = {c: rng.integers(-127, 128, size=c).astype(np.int8) for c in {s[1] for s in SHAPES}}
+    awr = awr_encode_all(mats)
+    nthreads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_pass(awr, x_by_cols, nthreads)
+    t0 = time.perf_counter()
+    nbytes = 0
+    for _ in range(args.steps):
+        nbytes += cpu_reference_pass(awr, x_by_cols, nthreads)
+    dt = time.perf_counter() - t0
+    value = nbytes / dt / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "7B-layer single-vector matvecs, ans-warp-rows layout (the reference's only "
+                                   "CPU-decodable layout): W_q 4096x4096, 11008x4096, 4096x11008 at sigma 4 and 2, "
+                                   "global CDF, B=1", "batch": 1, "seed": 20251203},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                             "sample": f"each step one pass over the 6 matrices with the oracle's C restatement "
+                                       f"of the reference decoder, {nthreads} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def time_graph(torch, fn, reps, inner=1):
+    """Capture fn() into a graph, replay `reps` times; returns ms per fn() call."""
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        fn()
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps / inner, g
+
+
+def copies_for(nbytes):
+    return int(min(64, max(2, -(-2 * L2_BYTES // max(1, nbytes)))))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from matvans_b200 import codec, ops
+
+    dev = torch.device("cuda", local)
+    mats = workload()
+    rng = np.random.default_rng(7)
+    x_by_cols = {c: rng.integers(-127, 128, size=c).astype(np.int8) for c in {s[1] for s in SHAPES}}
+    xd = {c: torch.from_numpy(v).to(dev) for c, v in x_by_cols.items()}
+
+    entries = []
+    for m in mats:
+        H = codec.entropy_bits(m["W"])
+        for local_cdf in (False, True):
+            M = ops.Q8Matrix.encode(m["W"], local=local_cdf, device=dev)
+            rows, cols = m["shape"]
+            entries.append(dict(name=f"{rows}x{cols}_s{int(m['sigma'])}_{'local' if local_cdf else 'global'}",
+                                M=M, rows=rows, cols=cols, sigma=m["sigma"], entropy=H,
+                                y=torch.empty((1, rows), dtype=torch.int32, device=dev),
+                                alg_bytes=M.payload_bytes + cols + 4 * rows))
+    # correctness gate before timing: bit-exact against the host int64 matvec
+    for e, m in zip(entries, [m for m in mats for _ in (0, 1)]):
+        y = e["M"].matvec(xd[e["cols"]][None], out=e["y"]).cpu().numpy()[0]
+        ref = (m["W"].astype(np.int32) @ x_by_cols[e["cols"]].astype(np.int32))
+        if not np.array_equal(y, ref):
+            raise SystemExit(f"bench: {e['name']} is not bit-exact")
+    ops.device_status()
+
+    def step():
+        for e in entries:
+            e["M"].matvec(xd[e["cols"]][None], out=e["y"])
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    _, g = time_graph(torch, step, 3)
+    for _ in range(max(args.warmup, 3)):
+        g.replay()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        e0.record()
+        for _ in range(args.steps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    step_bytes = sum(int8_equiv_bytes(e["rows"], e["cols"]) for e in entries)
+    value = world * step_bytes / (ms * 1e-3) / 1e9
+    alg = sum(e["alg_bytes"] for e in entries)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms * 1e-3) / 1e9
+    ops.device_status()
+
+    # per-matrix us/matvec with rotating copies (cold L2), and the comparators
+    per = {}
+    for e in entries:
+        M = e["M"]
+        R = copies_for(M.payload_bytes)
+        copies = [M] + [ops.Q8Matrix({"rows": M.rows, "cols": M.cols, "blocks": M.blocks.cpu().numpy(),
+                                      "blk_off": M.blk_off.cpu().numpy(),
+                                      "tbl": M.tbl.cpu().numpy().view(np.uint16),
+                                      "tbl_off": M.tbl_off.cpu().numpy(), "seg_quads": M.seg_quads,
+                                      "nseg": M.nseg, "local": M.local, "max_blk_rows": M.max_blk_rows,
+                                      "payload_bytes": M.payload_bytes, "bits_per_weight": M.bits_per_weight},
+                                     device=dev) for _ in range(R - 1)]
+        x1 = xd[e["cols"]][None]
+        t_ms, _ = time_graph(torch, lambda: [c.matvec(x1, out=e["y"]) for c in copies], 20, inner=R)
+        per[e["name"]] = {"us": 1e3 * t_ms, "int8_equiv_gbs": int8_equiv_bytes(e["rows"], e["cols"]) / t_ms / 1e6,
+                          "compressed_gbs": e["alg_bytes"] / t_ms / 1e6, "bits_per_weight": M.bits_per_weight,
+                          "entropy_bits": e["entropy"]}
+        del copies
+    torch.cuda.empty_cache()
+    dense, cublas, awr_t, wpr_t = {}, {}, {}, {}
+    for m in mats:
+        if m["sigma"] != 4.0:
+            continue
+        rows, cols = m["shape"]
+        key = f"{rows}x{cols}"
+        Wd = torch.from_numpy(m["W"]).to(dev)
+        R = copies_for(rows * cols)
+        Ws = [Wd] + [Wd.clone() for _ in range(R - 1)]
+        yd = torch.empty((1, rows), dtype=torch.int32, device=dev)
+        x1 = xd[cols][None]
+        t_ms, _ = time_graph(torch, lambda: [ops.dense_matvec(w, x1, out=yd) for w in Ws], 20, inner=R)
+        dense[key] = {"us": 1e3 * t_ms, "int8_equiv_gbs": int8_equiv_bytes(rows, cols) / t_ms / 1e6}
+        del Ws
+        Wf = Wd.float()
+        R = copies_for(4 * rows * cols)
+        Wfs = [Wf] + [Wf.clone() for _ in range(R - 1)]
+        xf = xd[cols].float()
+        t_ms, _ = time_graph(torch, lambda: [torch.mv(w, xf) for w in Wfs], 20, inner=R)
+        cublas[key] = {"us": 1e3 * t_ms}
+        del Wfs, Wf, Wd
+        A = ops.AwrMatrix.encode(m["W"], device=dev)
+        R = copies_for(4 * A.n_words)
+        As = [A] + [ops.AwrMatrix(A.compressed.cpu().numpy(), A.offsets.cpu().numpy(), A.ppf.cpu().numpy(),
+                                  A.ppf_cum.cpu().numpy(), A.ppf_prob.cpu().numpy(), rows, cols, dev)
+                    for _ in range(R - 1)]
+        t_ms, _ = time_graph(torch, lambda: [a.matvec(x1, out=yd) for a in As], 10, inner=R)
+        awr_t[key] = {"us": 1e3 * t_ms, "bits_per_weight": 32.0 * A.n_words / (rows * cols)}
+        del As, A
+        if cols % 512 == 0 and rows == cols:
+            P = ops.WprMatrix.encode(m["W"], device=dev)
+            R = copies_for(2 * P.payload_size)
+            from matvans_b200.codec import CompressedMatrix
+            cm = CompressedMatrix(rows, cols, 1.0, P.cursors.cpu().numpy(), P.min_value, P.cdf.cpu().numpy(),
+                                  P.ppf.cpu().numpy(), P.payload.cpu().numpy()[:P.payload_size])
+            Ps = [P] + [ops.WprMatrix(cm, dev) for _ in range(R - 1)]
+            t_ms, _ = time_graph(torch, lambda: [p.matvec(x1, out=yd) for p in Ps], 10, inner=R)
+            wpr_t[key] = {"us": 1e3 * t_ms, "bits_per_weight": 16.0 * P.payload_size / (rows * cols)}
+            del Ps, P
+        torch.cuda.empty_cache()
+
+    # end to end through the public API: pinned host x in, int32 y out, every step
+    xh = {c: torch.from_numpy(v).pin_memory() for c, v in x_by_cols.items()}
+    yh = [torch.empty((1, e["rows"]), dtype=torch.int32).pin_memory() for e in entries]
+    xin = {c: torch.empty((1, c), dtype=torch.int8, device=dev) for c in xh}
+
+    def e2e_step():
+        for c in xh:
+            xin[c].copy_(xh[c][None], non_blocking=True)
+        for e, h in zip(entries, yh):
+            e["M"].matvec(xin[e["cols"]], out=e["y"])
+            h.copy_(e["y"], non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / args.steps * 1e3
+    e2e_ms = max(e0.elapsed_time(e1) / args.steps, wall)
+    h2d = sum(x.numel() for x in xh.values())
+    d2h = sum(4 * e["rows"] for e in entries)
+
+    line = None
+    if rank == 0:
+        cb = None
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_baseline(mats, x_by_cols)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+            "config": {"workload": "7B-layer single-vector matvecs (Q8-stripe layout): W_q 4096x4096, 11008x4096, "
+                                   "4096x11008 at sigma 4 and 2, each with a global and a per-row CDF; 12 matvecs "
+                                   "per step, B=1, seeded synthetic int8 weights and x",
+                       "batch": 1, "matvecs_per_step": len(entries), "seed": 20251203,
+                       "l2": f"working set {alg / 2**20:.0f} MiB > 126 MiB L2, each matrix read once per step",
+                       "timing": "CUDA graph of one step, CUDA events over K replays, max over ranks"},
+            "us_per_matvec": {k: round(v["us"], 3) for k, v in per.items()},
+            "per_matrix": per,
+            "dense_dp4a": dense, "cublas_sgemv_fp32": cublas, "ans_warp_rows_kernel": awr_t,
+            "warp_per_row_kernel": wpr_t,
+            "speedup_vs_dense_dp4a": {k: round(dense[k.split("_s")[0]]["us"] / v["us"], 3)
+                                      for k, v in per.items() if k.split("_s")[0] in dense and "_s4_" in k},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "q8_kernel<1,false>",
+                         "note": "algorithmic bytes = compressed streams + tables + offsets + x + int32 y"},
+            "gpu_launches": args.steps * len(entries),
+            "clocks": sampler.summary(),
+            "e2e": {"value": world * step_bytes / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "cpu_baseline": cb,
+        }
+    del g
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

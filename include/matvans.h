@@ -1,0 +1,236 @@
+/*
+ * matvans.h -- C ABI of the B200 entropy-coded int8 matrix-vector product.
+ *
+ * An int8 weight matrix is stored as interleaved rANS streams and decoded
+ * inside the matvec kernel, so it never exists uncompressed in device memory.
+ * Three stream layouts are supported:
+ *
+ *   AWR  "ans-warp-rows": the reference's safetensors layout (7-bit quad rANS,
+ *        64-bit state, 32 lanes per row sharing one word stream), written by
+ *        buffered/encoder.py:394-511 and decoded by
+ *        buffered/ans-warp-rows-kernel.cu:7-221.
+ *   WPR  "matvansWarpPerRow": the reference's .bin layout (8-bit rANS, 32-bit
+ *        head, 16-bit words, one stream per lane), written by
+ *        matvansWarpPerRow/create_matrices_WarpPerRow.py:353-461 and decoded by
+ *        matvansWarpPerRow/matvansWarpPerRow-kernel.cu:46-175.
+ *   Q8   this library's own stripe layout (8-bit quad rANS with a 64-bit state;
+ *        lane = row of a 32-row stripe, rows cut into column segments; one
+ *        global table or one table per row).  No reference counterpart.
+ *
+ * Conventions
+ *   - Every function returns mv_status (0 = MV_OK); on failure
+ *     mv_last_error() returns a message for the calling thread.
+ *   - All pointers named *_dev are device pointers owned by the caller; the
+ *     library does not allocate on the launch paths except one lazily created
+ *     per-device status word (see mv_device_status).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *   - x is [batch][cols] int8 row-major; y is [batch][rows] int32.  y is
+ *     exact: decoded weights times x accumulated in int32.  y_scaled, when
+ *     non-NULL, is [batch][rows] float with y_scaled = (float)y * scale[row].
+ *   - Launches are asynchronous; device-side stream checks (overrun, final
+ *     state mismatch, wait timeout) raise bits in the per-device status word,
+ *     read and cleared by mv_device_status().
+ */
+#ifndef MATVANS_H
+#define MATVANS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int mv_status;
+#define MV_OK 0
+#define MV_ERR_ARG 1          /* invalid argument: NULL pointer, bad size      */
+#define MV_ERR_SHAPE 2        /* shape not representable in the layout         */
+#define MV_ERR_FORMAT 3       /* malformed file, tensor or stream              */
+#define MV_ERR_IO 4           /* file could not be read or written             */
+#define MV_ERR_CUDA 5         /* a CUDA runtime call failed                    */
+#define MV_ERR_DEVICE 6       /* a device-side check failed                    */
+#define MV_ERR_NOMEM 7        /* host allocation failed                        */
+#define MV_ERR_UNSUPPORTED 8  /* valid request this build does not implement   */
+
+/* Device status bits (mv_device_status). */
+#define MV_DEV_STREAM_OVERRUN 0x1u   /* a lane consumed more words than its stream holds */
+#define MV_DEV_FINAL_STATE 0x2u      /* a coder did not end in its initial state        */
+#define MV_DEV_WAIT_TIMEOUT 0x4u     /* a bounded wait on a copy or queue gave up       */
+#define MV_DEV_BAD_TABLE 0x8u        /* a probability table does not sum to 2^precision */
+
+const char *mv_version(void);
+const char *mv_last_error(void);
+
+/* Synchronises `stream`, then reads and clears the status word of the current
+ * device.  *flags receives the MV_DEV_* bits raised since the last call. */
+mv_status mv_device_status(void *stream, uint32_t *flags);
+
+/* ------------------------------------------------------------------ AWR --- */
+
+/* Replaces the host launcher mat_vec_mul_coalesced of
+ * buffered/ans-warp-rows.cu:38-60 (kernel signature ans-warp-rows-kernel.cu:7-17)
+ * with identical arguments and output: one int8 per row,
+ * clamp(round_half_even((float)y * scale)) as in ans-warp-rows-kernel.cu:212-220.
+ * Like the reference it returns nothing; errors print to stderr and are kept
+ * for mv_last_error().  Launches on the legacy default stream. */
+void mat_vec_mul_coalesced(const void *in_vector_gpu, void *out_vector_gpu, size_t in_dim,
+                           size_t out_dim, float scale, const void *compressed,
+                           const uint32_t *warp_offsets, const uint32_t *ppf,
+                           const uint32_t *ppf_cum, const uint32_t *ppf_prob);
+
+/* Exact int32 form of the same decode (the reference kernel's accumulator
+ * before its fused requantisation, ans-warp-rows-kernel.cu:191-210), for
+ * batch vectors.  n_words bounds every read of `compressed_dev` (u32 words,
+ * 16-byte aligned).  warp_offsets are in uint4 units (buffered/encoder.py:482).
+ * Requires cols % 128 == 0 (buffered/encoder.py:397). */
+mv_status mv_awr_matvec(const uint32_t *compressed_dev, size_t n_words,
+                        const uint32_t *warp_offsets_dev, const uint32_t *ppf_dev,
+                        const uint32_t *ppf_cum_dev, const uint32_t *ppf_prob_dev, int rows,
+                        int cols, const int8_t *x_dev, int batch, int32_t *y_dev,
+                        const float *row_scales_dev, float *y_scaled_dev, void *stream);
+
+/* Fused decode + dot product + requantisation to int8 for one vector, the
+ * chained step of buffered/ans-warp-rows.cu:208-221: out8[r] =
+ * clamp(round_half_even((float)y[r] * scale), -128, 127). */
+mv_status mv_awr_matvec_requant(const uint32_t *compressed_dev, size_t n_words,
+                                const uint32_t *warp_offsets_dev, const uint32_t *ppf_dev,
+                                const uint32_t *ppf_cum_dev, const uint32_t *ppf_prob_dev,
+                                int rows, int cols, const int8_t *x_dev, float scale,
+                                int8_t *out8_dev, void *stream);
+
+/* ------------------------------------------------------------------ WPR --- */
+
+/* Replaces the kernel launch in CompressedMatrix::decompressAndMult,
+ * matvansWarpPerRow/matvansWarpPerRow.cu:150-164 (kernel arguments of
+ * matvansWarpPerRow-kernel.cu:46-50): int32 y for `batch` vectors.
+ * `payload_dev` holds payload_size u16 words (16-byte aligned), `cursors_dev`
+ * the per-row u16 cursors, `cdf_dev` G+1 low cdf bytes, `ppf_dev` 256 bytes.
+ * Requires cols % 512 == 0 (create_matrices_WarpPerRow.py:361-366). */
+mv_status mv_wpr_matvec(const uint16_t *payload_dev, size_t payload_size,
+                        const uint32_t *cursors_dev, int8_t min_value, const uint8_t *cdf_dev,
+                        int G, const uint8_t *ppf_dev, int rows, int cols, const int8_t *x_dev,
+                        int batch, int32_t *y_dev, const float *row_scales_dev,
+                        float *y_scaled_dev, void *stream);
+
+/* The epilogue of matvansWarpPerRow.cu:51-72,167-172 fused into one kernel
+ * without a host round trip: delta = max|y|/127 (fp32), out8[r] =
+ * (int8)round_half_even((float)y[r] / delta), no clamp (as in the reference).
+ * `absmax_scratch_dev` is one caller-owned uint32.  Writes delta to
+ * *delta_dev. */
+mv_status mv_requant_absmax(const int32_t *y_dev, int n, int8_t *out8_dev, float *delta_dev,
+                            uint32_t *absmax_scratch_dev, void *stream);
+
+/* ------------------------------------------------------------------- Q8 --- */
+
+/* Device view of one Q8-stripe matrix (all pointers are device pointers).
+ * Layout (built by mv_q8_encode):
+ *   stripes = ceil(rows/32), nseg = ceil(ceil(cols/4) / seg_quads).
+ *   Block b = stripe*nseg + seg starts at blocks + 32*blk_off[b] (128-byte
+ *   units) and spans blk_off[b+1]-blk_off[b] word-rows of 32 u32: word-row 0
+ *   and 1 hold the low / high halves of the 32 lanes' 64-bit coder states,
+ *   word-row 2+k holds the k-th refill word of each lane (lane = row within
+ *   the stripe).
+ *   Table t (t = row if local, else 0) is tbl[tbl_off[t] .. tbl_off[t+1]) of
+ *   u16 entries (uint8 symbol | freq << 8), sorted by symbol, freqs summing to
+ *   256.  Rows past `rows` in the last stripe use table tbl_pad (local mode).
+ */
+typedef struct mv_q8_view {
+    const uint32_t *blocks;
+    const uint32_t *blk_off;  /* [stripes*nseg + 1] */
+    const uint16_t *tbl;
+    const uint32_t *tbl_off;  /* [ntables + 1] */
+    int32_t rows, cols;
+    int32_t seg_quads;        /* quads (4 columns) per lane per segment     */
+    int32_t nseg;
+    int32_t local;            /* 1 = one table per (padded) row, 0 = global  */
+    int32_t max_blk_rows;     /* max word-rows of any block                  */
+    uint32_t blocks_rows;     /* word-rows (128 bytes) readable at `blocks`  */
+    uint32_t tbl_len;         /* u16 entries readable at `tbl`               */
+} mv_q8_view;
+
+/* y = W x for any batch >= 1 (passes of up to 16 vectors share one decode). */
+mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int32_t *y_dev,
+                       const float *row_scales_dev, float *y_scaled_dev, void *stream);
+
+/* Decode the whole matrix to W_dev[rows][cols] (test / debugging aid). */
+mv_status mv_q8_decode(const mv_q8_view *m, int8_t *W_dev, void *stream);
+
+/* ---------------------------------------------------------------- dense --- */
+
+/* Dense int8 comparator: y = W x with W int8 row-major [rows][cols] in device
+ * memory (the baseline of baselines/baseline_int8/baseline_matVec_custom.cu:99-155,
+ * written for sm_100a).  cols % 16 == 0. */
+mv_status mv_dense_matvec(const int8_t *W_dev, int rows, int cols, const int8_t *x_dev,
+                          int batch, int32_t *y_dev, void *stream);
+
+/* ------------------------------------------------------ host: encoders --- */
+
+/* Encoders produce a blob: a set of named host arrays. */
+typedef struct mv_blob mv_blob;
+void mv_blob_free(mv_blob *b);
+/* Looks up array `name`; *data points into the blob (valid until freed). */
+mv_status mv_blob_get(const mv_blob *b, const char *name, const void **data, size_t *nbytes);
+/* Scalar metadata stored in the blob (e.g. "rows", "min_value"). */
+mv_status mv_blob_get_i64(const mv_blob *b, const char *name, int64_t *value);
+/* Name of the i-th array (NULL past the end). */
+const char *mv_blob_name(const mv_blob *b, int i);
+
+/* Reference-compatible AWR encoder: byte-identical to
+ * compress_ans_warp_rows(W, 32) of buffered/encoder.py:394-461 with the model
+ * of fit_128bit_encoder_model (:271-306).  Arrays: "compressed" u32,
+ * "warp_offsets" u32[rows] (uint4 units), "cdf" u8, "ppf"/"ppf_cum"/"ppf_prob"
+ * u32[32] (encoder.py:309-320,464-470); scalars "min_value", "rows", "cols".
+ * Fails with MV_ERR_SHAPE unless cols % 128 == 0, and MV_ERR_UNSUPPORTED for
+ * more than 128 distinct values (encoder.py:303). */
+mv_status mv_awr_encode(const int8_t *W, int rows, int cols, int nthreads, mv_blob **out);
+
+/* Reference-compatible WPR encoder: encode_matrix of
+ * create_matrices_WarpPerRow.py:353-430 with create_entropy_model (:131-187)
+ * and create_ppf (:189-208); padding words are zero.  Arrays: "payload" u16,
+ * "cursors" u32[rows], "cdf" u8[G+1] (low bytes), "ppf" u8[256]; scalars
+ * "min_value", "G", "rows", "cols".  cols % 512 == 0. */
+mv_status mv_wpr_encode(const int8_t *W, int rows, int cols, int nthreads, mv_blob **out);
+
+/* Q8-stripe encoder.  local = 1 fits one table per row, 0 one table for the
+ * matrix.  seg_quads = 0 picks the segment length automatically.  Arrays:
+ * "blocks" u32, "blk_off" u32, "tbl" u16, "tbl_off" u32; scalars "rows",
+ * "cols", "seg_quads", "nseg", "local", "max_blk_rows", "payload_bytes"
+ * (blocks + tables + offsets). */
+mv_status mv_q8_encode(const int8_t *W, int rows, int cols, int local, int seg_quads,
+                       int nthreads, mv_blob **out);
+
+/* --------------------------------------------------------- host: files --- */
+
+/* Reads a safetensors file into a blob (one array per tensor; scalar
+ * "<name>.ndim" and "<name>.shape<i>" entries give the shapes; dtype codes in
+ * "<name>.dtype": 1 i8, 2 u8, 3 i16, 4 u16, 5 i32, 6 u32, 7 f32, 8 i64, 9 u64,
+ * 10 f64).  Replaces SaneSafetensorFile (buffered/sane_safetensors.hpp:17-68). */
+mv_status mv_read_safetensors(const char *path, mv_blob **out);
+
+/* Writes the arrays of `b` as a safetensors file (shapes and dtypes from the
+ * same scalar entries). */
+mv_status mv_write_safetensors(const char *path, const mv_blob *b);
+
+/* Reads a matvansWarpPerRow .bin file (create_matrices_WarpPerRow.py:440-461,
+ * matvansWarpPerRow.cu:225-258).  Scalars "num_matrices", "result_hash",
+ * "max_word_count", "len_v"; array "vector"; per matrix i arrays
+ * "m<i>.cursors", "m<i>.cdf", "m<i>.ppf", "m<i>.payload" and scalars
+ * "m<i>.rows", "m<i>.cols", "m<i>.min_value", "m<i>.G", "m<i>.payload_size". */
+mv_status mv_read_wpr_bin(const char *path, mv_blob **out);
+
+/* Fault injection for tests of the device-side error paths (no reference
+ * counterpart).  MV_INJECT_WAIT_LIMIT sets the iteration bound of every
+ * shared-memory barrier wait (0 restores the default); MV_INJECT_DROP_COPY
+ * (value 1) makes Q8 launches skip their bulk copies, so their bounded waits
+ * run out and raise MV_DEV_WAIT_TIMEOUT.  Process-wide, not thread-safe. */
+#define MV_INJECT_WAIT_LIMIT 1
+#define MV_INJECT_DROP_COPY 2
+mv_status mv_debug_inject(int what, uint32_t value);
+
+/* FxHash-style hash of an int8 vector (buffered/encoder.py:8-20). */
+uint32_t mv_hash_int8(const int8_t *v, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MATVANS_H */

@@ -1,0 +1,157 @@
+"""ctypes binding of libmatvans.so (the C ABI declared in include/matvans.h).
+
+The shared library is built in-tree by ``python -m matvans_b200.build`` (or
+``__graft_entry__.build()``).  Nothing here falls back to another
+implementation: if the library is missing, loading raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmatvans.so")
+
+MV_OK = 0
+STATUS_NAMES = {1: "MV_ERR_ARG", 2: "MV_ERR_SHAPE", 3: "MV_ERR_FORMAT", 4: "MV_ERR_IO", 5: "MV_ERR_CUDA",
+                6: "MV_ERR_DEVICE", 7: "MV_ERR_NOMEM", 8: "MV_ERR_UNSUPPORTED"}
+DEV_STREAM_OVERRUN, DEV_FINAL_STATE, DEV_WAIT_TIMEOUT, DEV_BAD_TABLE = 1, 2, 4, 8
+
+# every symbol include/matvans.h declares
+EXPORTS = [
+    "mv_version", "mv_last_error", "mv_device_status", "mat_vec_mul_coalesced", "mv_awr_matvec",
+    "mv_awr_matvec_requant", "mv_wpr_matvec", "mv_requant_absmax", "mv_q8_matvec", "mv_q8_decode",
+    "mv_dense_matvec", "mv_blob_free", "mv_blob_get", "mv_blob_get_i64", "mv_blob_name", "mv_awr_encode",
+    "mv_wpr_encode", "mv_q8_encode", "mv_read_safetensors", "mv_write_safetensors", "mv_read_wpr_bin",
+    "mv_hash_int8", "mv_debug_inject",
+]
+
+
+class MatvansError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Q8View(ctypes.Structure):
+    """struct mv_q8_view (include/matvans.h)."""
+    _fields_ = [("blocks", ctypes.c_void_p), ("blk_off", ctypes.c_void_p), ("tbl", ctypes.c_void_p),
+                ("tbl_off", ctypes.c_void_p), ("rows", ctypes.c_int32), ("cols", ctypes.c_int32),
+                ("seg_quads", ctypes.c_int32), ("nseg", ctypes.c_int32), ("local", ctypes.c_int32),
+                ("max_blk_rows", ctypes.c_int32), ("blocks_rows", ctypes.c_uint32),
+                ("tbl_len", ctypes.c_uint32)]
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m matvans_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, i32, sz, u32p = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p
+    st = ctypes.c_int
+    sig = {
+        "mv_version": ([], ctypes.c_char_p),
+        "mv_last_error": ([], ctypes.c_char_p),
+        "mv_device_status": ([P, ctypes.POINTER(ctypes.c_uint32)], st),
+        "mat_vec_mul_coalesced": ([P, P, sz, sz, ctypes.c_float, P, P, P, P, P], None),
+        "mv_awr_matvec": ([P, sz, P, P, P, P, i32, i32, P, i32, P, P, P, P], st),
+        "mv_awr_matvec_requant": ([P, sz, P, P, P, P, i32, i32, P, ctypes.c_float, P, P], st),
+        "mv_wpr_matvec": ([P, sz, P, ctypes.c_int8, P, i32, P, i32, i32, P, i32, P, P, P, P], st),
+        "mv_requant_absmax": ([P, i32, P, P, P, P], st),
+        "mv_q8_matvec": ([ctypes.POINTER(Q8View), P, i32, P, P, P, P], st),
+        "mv_q8_decode": ([ctypes.POINTER(Q8View), P, P], st),
+        "mv_dense_matvec": ([P, i32, i32, P, i32, P, P], st),
+        "mv_blob_free": ([P], None),
+        "mv_blob_get": ([P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)], st),
+        "mv_blob_get_i64": ([P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)], st),
+        "mv_blob_name": ([P, i32], ctypes.c_char_p),
+        "mv_awr_encode": ([P, i32, i32, i32, ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_wpr_encode": ([P, i32, i32, i32, ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_q8_encode": ([P, i32, i32, i32, i32, i32, ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_read_safetensors": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_write_safetensors": ([ctypes.c_char_p, P], st),
+        "mv_read_wpr_bin": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_hash_int8": ([P, sz], ctypes.c_uint32),
+        "mv_debug_inject": ([i32, ctypes.c_uint32], st),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = L
+    return L
+
+
+def check(rc):
+    if rc != MV_OK:
+        raise MatvansError(rc, lib().mv_last_error().decode())
+
+
+# ---------------------------------------------------------------- blobs
+
+_DT = {1: np.int8, 2: np.uint8, 3: np.int16, 4: np.uint16, 5: np.int32, 6: np.uint32, 7: np.float32,
+       8: np.int64, 9: np.uint64, 10: np.float64}
+_DT_CODE = {np.dtype(v): k for k, v in _DT.items()}
+
+
+class Blob:
+    """Host arrays + scalars produced by an encoder or a file reader."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _LIB is not None:
+            _LIB.mv_blob_free(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def names(self):
+        out, i = [], 0
+        while True:
+            n = lib().mv_blob_name(self._h, i)
+            if n is None:
+                return out
+            out.append(n.decode())
+            i += 1
+
+    def scalar(self, name):
+        v = ctypes.c_int64()
+        check(lib().mv_blob_get_i64(self._h, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    def has_scalar(self, name):
+        v = ctypes.c_int64()
+        return lib().mv_blob_get_i64(self._h, name.encode(), ctypes.byref(v)) == MV_OK
+
+    def array(self, name, dtype=None):
+        p, n = ctypes.c_void_p(), ctypes.c_size_t()
+        check(lib().mv_blob_get(self._h, name.encode(), ctypes.byref(p), ctypes.byref(n)))
+        if dtype is None:
+            dtype = _DT[self.scalar(name + ".dtype")] if self.has_scalar(name + ".dtype") else np.uint8
+        if n.value == 0:
+            a = np.zeros(0, dtype=dtype)
+        else:
+            buf = (ctypes.c_uint8 * n.value).from_address(p.value)
+            a = np.frombuffer(buf, dtype=np.uint8).copy().view(dtype)
+        if self.has_scalar(name + ".ndim"):
+            nd = self.scalar(name + ".ndim")
+            shape = tuple(self.scalar(f"{name}.shape{i}") for i in range(nd))
+            if int(np.prod(shape)) == a.size:
+                a = a.reshape(shape)
+        return a
+
+
+def ptr(a):
+    """Address of a numpy array or torch tensor."""
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def new_blob_out():
+    return ctypes.c_void_p()

@@ -1,0 +1,289 @@
+// Decode + int8 matvec for the reference's "ans-warp-rows" (AWR) layout on
+// sm_100a.  Parity target: buffered/ans-warp-rows-kernel.cu:7-221.
+//
+// The layout makes the 32 lanes of a row share one word stream: at every quad
+// step the lanes whose 64-bit state dropped below 2^32 take the next words in
+// lane order (ballot + prefix popcount), from a 128-word warp-wide cache that
+// holds one uint4 per lane and is read field by field (x, then y, z, w) --
+// see ans-warp-rows-kernel.cu:76-139.  That consumption order is part of the
+// format, so this kernel keeps one warp per row and reproduces it exactly.
+// What changes on B200:
+//   * the three 32-entry packed tables are expanded once per CTA into a
+//     128-quantile x 32-lane shared table (entry (q,l) at word q*32 + l), so
+//     the four lookups of a quad are four conflict-free loads instead of
+//     twelve warp shuffles (ans-warp-rows-kernel.cu:147-189);
+//   * the warp cache advances lazily: a block is loaded only when a lane
+//     actually consumes one of its words (the reference also reloads when the
+//     cursor lands exactly on a block boundary, which can read past the row);
+//   * when the stream length is known, the next block is prefetched one block
+//     ahead and every load is bounds-checked;
+//   * any number of vectors per pass (1..16) share one decode, x is staged
+//     once per CTA, and the int32 result is exact (requantisation optional).
+#include <algorithm>
+#include <cstdio>
+
+#include "mv_device.cuh"
+
+namespace mv {
+
+struct AwrLaunch {
+    const uint4 *comp;
+    size_t n_u4;  // 0 = unknown (reference shim): no prefetch, no bounds checks
+    const uint32_t *offs, *ppf, *cum, *prob;
+    int rows, cols;
+    const int8_t *x;
+    int batch;
+    int32_t *y;
+    const float *scales;
+    float *ys;
+    int8_t *out8;  // requantised output (one vector)
+    float scale;
+    uint32_t *status;
+};
+
+template <int NV, bool REQUANT>
+__global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t *lut = reinterpret_cast<uint32_t *>(smem);  // 128 * 32 words
+    uint32_t *xs = lut + 128 * 32;                       // [cols/4][NV]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
+    const int nq = L.cols >> 2;
+
+    for (int i = threadIdx.x; i < 128 * 32; i += blockDim.x) {
+        const uint32_t q = (uint32_t)i >> 5, sh = 8 * (q & 3);
+        const uint32_t sym = (__ldg(L.ppf + (q >> 2)) >> sh) & 0xFF;
+        const uint32_t c = (__ldg(L.cum + (q >> 2)) >> sh) & 0xFF;
+        const uint32_t p = (__ldg(L.prob + (q >> 2)) >> sh) & 0xFF;
+        if (c > q || p == 0) atomicOr(L.status, MV_DEV_BAD_TABLE);
+        lut[i] = sym | (p << 8) | (((q - c) & 0xFFFF) << 16);
+    }
+    const bool xal = (reinterpret_cast<uintptr_t>(L.x) & 3) == 0;
+    for (int i = threadIdx.x; i < nq * NV; i += blockDim.x) {
+        const int c = i / NV, v = i % NV;
+        uint32_t val = 0;
+        if (v < L.batch) {
+            const int8_t *p = L.x + (size_t)v * L.cols + 4 * c;
+            if (xal) val = *reinterpret_cast<const uint32_t *>(p);
+            else for (int j = 0; j < 4; j++) val |= (uint32_t)(uint8_t)p[j] << (8 * j);
+        }
+        xs[i] = val;
+    }
+    __syncthreads();
+
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t *lut_l = lut + lane;
+    const bool bounded = L.n_u4 != 0;
+
+    for (int row = blockIdx.x * W + warp; row < L.rows; row += gridDim.x * W) {
+        size_t bi = __ldg(L.offs + row);  // uint4 index of the block held in `cache`
+        uint4 cache = make_uint4(0, 0, 0, 0), nxt = make_uint4(0, 0, 0, 0);
+        bool ovf = false;
+        if (!bounded || bi + 32 <= L.n_u4) cache = L.comp[bi + lane];
+        else ovf = true;
+        if (bounded && bi + 64 <= L.n_u4) nxt = L.comp[bi + 32 + lane];
+        unsigned long long state = ((unsigned long long)cache.w << 32) | cache.z;
+        uint32_t wcc = 64;  // reference cursor into the 128-word cache
+        bool lag = false;   // cursor crossed a 32-word boundary without advancing
+
+        auto advance = [&](uint32_t leaving_gen) {
+            if (leaving_gen == 3) {  // next block
+                bi += 32;
+                if (bounded) {
+                    if (bi + 32 > L.n_u4) ovf = true;
+                    cache = nxt;
+                    nxt = (bi + 64 <= L.n_u4) ? L.comp[bi + 32 + lane] : make_uint4(0, 0, 0, 0);
+                } else {
+                    cache = L.comp[bi + lane];
+                }
+            } else {
+                cache.x = cache.y;
+                cache.y = cache.z;
+                cache.z = cache.w;
+            }
+        };
+
+        int acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = 0;
+
+        for (int j = 0; j < nq; j += 32) {
+            const bool need = (state >> 32) == 0;
+            const uint32_t ballot = __ballot_sync(0xffffffffu, need);
+            if (ballot) {
+                if (lag) {
+                    advance((wcc >> 5) == 0 ? 3u : 0u);
+                    lag = false;
+                }
+                const uint32_t off = __popc(ballot & lt_mask);
+                const uint32_t num = __popc(ballot);
+                const uint32_t lc = (wcc + off) & 31;
+                const uint32_t gen = wcc >> 5;
+                uint32_t rv = __shfl_sync(0xffffffffu, cache.x, lc);
+                if (((wcc + num - 1) >> 5) != gen) {
+                    advance(gen);
+                    const uint32_t rv2 = __shfl_sync(0xffffffffu, cache.x, lc);
+                    if (((wcc + off) >> 5) != gen) rv = rv2;
+                } else if (((wcc + num) >> 5) != gen) {
+                    lag = true;
+                }
+                if (need) state = (state << 32) | rv;
+                wcc = (wcc + num) & 127;
+            }
+            const uint32_t lo = (uint32_t)state;
+            const uint32_t e0 = lut_l[(lo & 0x7Fu) << 5];
+            const uint32_t e1 = lut_l[((lo >> 7) & 0x7Fu) << 5];
+            const uint32_t e2 = lut_l[((lo >> 14) & 0x7Fu) << 5];
+            const uint32_t e3 = lut_l[((lo >> 21) & 0x7Fu) << 5];
+            const uint32_t p0 = __byte_perm(e0, 0, 0x4441), p1 = __byte_perm(e1, 0, 0x4441);
+            const uint32_t p2 = __byte_perm(e2, 0, 0x4441), p3 = __byte_perm(e3, 0, 0x4441);
+            const uint32_t p01 = p0 * p1, p012 = p01 * p2, p0123 = p012 * p3;
+            const uint32_t ns = (e0 >> 16) + p0 * (e1 >> 16) + p01 * (e2 >> 16) + p012 * (e3 >> 16);
+            state = (state >> 28) * (unsigned long long)p0123 + ns;
+            const uint32_t wq =
+                __byte_perm(__byte_perm(e0, e1, 0x0040), __byte_perm(e2, e3, 0x0040), 0x5410);
+            const uint32_t *xq = xs + (j + lane) * NV;
+#pragma unroll
+            for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wq, (int)xq[v], acc[v]);
+        }
+        if (ovf) atomicOr(L.status, MV_DEV_STREAM_OVERRUN);
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+        }
+        if (lane == 0) {
+            if (REQUANT) {
+                // ans-warp-rows-kernel.cu:212-220
+                const int r = __float2int_rn((float)acc[0] * L.scale);
+                L.out8[row] = (int8_t)max(-128, min(127, r));
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; v++)
+                    if (v < L.batch) {
+                        L.y[(size_t)v * L.rows + row] = acc[v];
+                        if (L.ys) L.ys[(size_t)v * L.rows + row] = (float)acc[v] * L.scales[row];
+                    }
+            }
+        }
+    }
+}
+
+namespace {
+
+template <int NV, bool REQUANT>
+mv_status launch_awr(const AwrLaunch &L, cudaStream_t st) {
+    const int W = 8;
+    const size_t smem = 128 * 32 * 4 + (size_t)(L.cols / 4) * NV * 4;
+    if (smem > (size_t)max_smem_optin())
+        return fail(MV_ERR_UNSUPPORTED, "AWR: %d columns x %d vectors exceed shared memory", L.cols, NV);
+    auto kern = awr_kernel<NV, REQUANT>;
+    int blocks_per_sm = 0;
+    mv_status rc = prepare_kernel((const void *)kern, smem, 32 * W, &blocks_per_sm);
+    if (rc) return rc;
+    const int want = (L.rows + W - 1) / W;
+    const int grid = std::max(1, std::min(want, std::max(1, blocks_per_sm) * sm_count()));
+    kern<<<grid, 32 * W, smem, st>>>(L);
+    MV_CUDA_TRY(cudaGetLastError(), "awr kernel launch");
+    return MV_OK;
+}
+
+mv_status awr_common(const uint32_t *comp, size_t n_words, const uint32_t *offs, const uint32_t *ppf,
+                     const uint32_t *cum, const uint32_t *prob, int rows, int cols, const int8_t *x,
+                     AwrLaunch &L) {
+    if (!comp || !offs || !ppf || !cum || !prob || !x) return fail(MV_ERR_ARG, "mv_awr: NULL pointer");
+    if (rows <= 0 || cols <= 0) return fail(MV_ERR_ARG, "mv_awr: rows/cols must be positive");
+    if (cols % 128) return fail(MV_ERR_SHAPE, "AWR layout needs cols %% 128 == 0 (cols=%d)", cols);
+    if (((uintptr_t)comp & 15) != 0) return fail(MV_ERR_ARG, "mv_awr: compressed not 16-byte aligned");
+    mv_status rc;
+    L.status = device_status_word(&rc);
+    if (rc) return rc;
+    L.comp = reinterpret_cast<const uint4 *>(comp);
+    L.n_u4 = n_words / 4;
+    L.offs = offs;
+    L.ppf = ppf;
+    L.cum = cum;
+    L.prob = prob;
+    L.rows = rows;
+    L.cols = cols;
+    L.x = x;
+    return MV_OK;
+}
+
+}  // namespace
+
+mv_status awr_matvec(const uint32_t *comp, size_t n_words, const uint32_t *offs, const uint32_t *ppf,
+                     const uint32_t *cum, const uint32_t *prob, int rows, int cols, const int8_t *x,
+                     int batch, int32_t *y, const float *scales, float *ys, cudaStream_t st) {
+    AwrLaunch L{};
+    mv_status rc = awr_common(comp, n_words, offs, ppf, cum, prob, rows, cols, x, L);
+    if (rc) return rc;
+    if (!y || batch <= 0) return fail(MV_ERR_ARG, "mv_awr_matvec: bad y/batch");
+    if (n_words == 0) return fail(MV_ERR_ARG, "mv_awr_matvec: n_words must be given");
+    if (ys && !scales) return fail(MV_ERR_ARG, "mv_awr_matvec: y_scaled needs row scales");
+    for (int v0 = 0; v0 < batch; v0 += 16) {
+        const int nb = std::min(16, batch - v0);
+        AwrLaunch P = L;
+        P.x = x + (size_t)v0 * cols;
+        P.batch = nb;
+        P.y = y + (size_t)v0 * rows;
+        P.scales = scales;
+        P.ys = ys ? ys + (size_t)v0 * rows : nullptr;
+        if (nb == 1) rc = launch_awr<1, false>(P, st);
+        else if (nb == 2) rc = launch_awr<2, false>(P, st);
+        else if (nb <= 4) rc = launch_awr<4, false>(P, st);
+        else if (nb <= 8) rc = launch_awr<8, false>(P, st);
+        else rc = launch_awr<16, false>(P, st);
+        if (rc) return rc;
+    }
+    return MV_OK;
+}
+
+mv_status awr_requant(const uint32_t *comp, size_t n_words, const uint32_t *offs, const uint32_t *ppf,
+                      const uint32_t *cum, const uint32_t *prob, int rows, int cols, const int8_t *x,
+                      float scale, int8_t *out8, cudaStream_t st) {
+    AwrLaunch L{};
+    mv_status rc = awr_common(comp, n_words, offs, ppf, cum, prob, rows, cols, x, L);
+    if (rc) return rc;
+    if (!out8) return fail(MV_ERR_ARG, "mv_awr_matvec_requant: NULL output");
+    L.batch = 1;
+    L.out8 = out8;
+    L.scale = scale;
+    return launch_awr<1, true>(L, st);
+}
+
+}  // namespace mv
+
+extern "C" {
+
+mv_status mv_awr_matvec(const uint32_t *compressed_dev, size_t n_words, const uint32_t *warp_offsets_dev,
+                        const uint32_t *ppf_dev, const uint32_t *ppf_cum_dev,
+                        const uint32_t *ppf_prob_dev, int rows, int cols, const int8_t *x_dev,
+                        int batch, int32_t *y_dev, const float *row_scales_dev, float *y_scaled_dev,
+                        void *stream) {
+    return mv::awr_matvec(compressed_dev, n_words, warp_offsets_dev, ppf_dev, ppf_cum_dev, ppf_prob_dev,
+                          rows, cols, x_dev, batch, y_dev, row_scales_dev, y_scaled_dev,
+                          (cudaStream_t)stream);
+}
+
+mv_status mv_awr_matvec_requant(const uint32_t *compressed_dev, size_t n_words,
+                                const uint32_t *warp_offsets_dev, const uint32_t *ppf_dev,
+                                const uint32_t *ppf_cum_dev, const uint32_t *ppf_prob_dev, int rows,
+                                int cols, const int8_t *x_dev, float scale, int8_t *out8_dev,
+                                void *stream) {
+    return mv::awr_requant(compressed_dev, n_words, warp_offsets_dev, ppf_dev, ppf_cum_dev, ppf_prob_dev,
+                           rows, cols, x_dev, scale, out8_dev, (cudaStream_t)stream);
+}
+
+// buffered/ans-warp-rows.cu:38-60: same arguments, same int8 output, legacy
+// default stream.  The stream length is unknown here, so no bounds checks.
+void mat_vec_mul_coalesced(const void *in_vector_gpu, void *out_vector_gpu, size_t in_dim, size_t out_dim,
+                           float scale, const void *compressed, const uint32_t *warp_offsets,
+                           const uint32_t *ppf, const uint32_t *ppf_cum, const uint32_t *ppf_prob) {
+    mv_status rc = mv::awr_requant(reinterpret_cast<const uint32_t *>(compressed), 0, warp_offsets, ppf,
+                                   ppf_cum, ppf_prob, (int)out_dim, (int)in_dim,
+                                   reinterpret_cast<const int8_t *>(in_vector_gpu), scale,
+                                   reinterpret_cast<int8_t *>(out_vector_gpu), 0);
+    if (rc) std::fprintf(stderr, "mat_vec_mul_coalesced: %s\n", mv_last_error());
+}
+
+}  // extern "C"

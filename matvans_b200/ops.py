@@ -1,0 +1,211 @@
+"""Device-side API: compressed matrices resident in GPU memory and the fused
+decode + matvec launches of libmatvans.so.
+
+torch provides device memory and the current CUDA stream; every launch goes
+through the C ABI.  There is no CPU or torch fallback: without a GPU or
+without the built library these calls raise.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import Q8View, check, lib
+
+_STATUS_BITS = {1: "stream overrun", 2: "final coder state mismatch", 4: "wait timeout", 8: "bad table"}
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev(a, device, dtype=None):
+    """numpy -> device tensor (16-byte aligned by the caching allocator)."""
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.view(dtype)
+    return t.to(device)
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _as_x(x, cols, device):
+    if not isinstance(x, torch.Tensor):
+        x = torch.from_numpy(np.ascontiguousarray(x, dtype=np.int8))
+    if x.dtype != torch.int8:
+        raise TypeError("x must be int8")
+    squeeze = x.dim() == 1
+    x2 = x.reshape(1, -1) if squeeze else x
+    if x2.shape[-1] != cols:
+        raise ValueError(f"x has {x2.shape[-1]} columns, matrix has {cols}")
+    return x2.to(device).contiguous(), squeeze
+
+
+def device_status(raise_on_error=True):
+    """Synchronise the current stream and read/clear the device status bits."""
+    flags = ctypes.c_uint32(0)
+    rc = lib().mv_device_status(_stream(), ctypes.byref(flags))
+    if rc not in (0, 6):
+        check(rc)
+    if flags.value and raise_on_error:
+        names = [n for b, n in _STATUS_BITS.items() if flags.value & b]
+        raise _lib.MatvansError(6, "device checks failed: " + ", ".join(names))
+    return flags.value
+
+
+class _Matrix:
+    rows: int
+    cols: int
+
+    def matvec(self, x, scales=None, out=None, out_scaled=None):
+        x2, squeeze = _as_x(x, self.cols, self.device)
+        B = x2.shape[0]
+        y = out if out is not None else torch.empty((B, self.rows), dtype=torch.int32, device=self.device)
+        ys = None
+        if scales is not None:
+            scales = scales if isinstance(scales, torch.Tensor) else torch.from_numpy(np.asarray(scales, np.float32))
+            scales = scales.to(self.device, torch.float32).contiguous()
+            ys = out_scaled if out_scaled is not None else torch.empty((B, self.rows), dtype=torch.float32,
+                                                                      device=self.device)
+        self._launch(x2, B, y, scales, ys)
+        if squeeze:
+            return (y[0], ys[0]) if ys is not None else y[0]
+        return (y, ys) if ys is not None else y
+
+
+class AwrMatrix(_Matrix):
+    """A matrix in the reference's ans-warp-rows layout (buffered/encoder.py:394-461)."""
+
+    def __init__(self, compressed, warp_offsets, ppf, ppf_cum, ppf_prob, rows, cols, device="cuda"):
+        self.device = torch.device(device)
+        self.rows, self.cols = int(rows), int(cols)
+        self.compressed = _dev(np.asarray(compressed, np.uint32), self.device)
+        self.offsets = _dev(np.asarray(warp_offsets, np.uint32), self.device)
+        self.ppf = _dev(np.asarray(ppf, np.uint32), self.device)
+        self.ppf_cum = _dev(np.asarray(ppf_cum, np.uint32), self.device)
+        self.ppf_prob = _dev(np.asarray(ppf_prob, np.uint32), self.device)
+        self.n_words = int(np.asarray(compressed).size)
+
+    @classmethod
+    def encode(cls, W, device="cuda"):
+        from . import codec
+        comp, offs, mn, cdf = codec.compress_ans_warp_rows(W, 32)
+        p, pc, pp = codec.decoder_model_from_128bit_encoder_model(mn, cdf)
+        return cls(comp, offs, codec.pack_4bytes(p), codec.pack_4bytes(pc), codec.pack_4bytes(pp),
+                   W.shape[0], W.shape[1], device)
+
+    @property
+    def payload_bytes(self):
+        return 4 * self.n_words + 4 * self.rows + 3 * 128
+
+    def _launch(self, x2, B, y, scales, ys):
+        check(lib().mv_awr_matvec(_p(self.compressed), self.n_words, _p(self.offsets), _p(self.ppf),
+                                  _p(self.ppf_cum), _p(self.ppf_prob), self.rows, self.cols, _p(x2), B, _p(y),
+                                  _p(scales), _p(ys), _stream()))
+
+    def matvec_requant(self, x, scale, out=None):
+        """Fused int8 output of ans-warp-rows-kernel.cu:212-220."""
+        x2, _ = _as_x(x, self.cols, self.device)
+        out = out if out is not None else torch.empty(self.rows, dtype=torch.int8, device=self.device)
+        check(lib().mv_awr_matvec_requant(_p(self.compressed), self.n_words, _p(self.offsets), _p(self.ppf),
+                                          _p(self.ppf_cum), _p(self.ppf_prob), self.rows, self.cols, _p(x2),
+                                          ctypes.c_float(scale), _p(out), _stream()))
+        return out
+
+
+class WprMatrix(_Matrix):
+    """A matrix in the reference's matvansWarpPerRow .bin layout."""
+
+    def __init__(self, cm, device="cuda"):
+        self.device = torch.device(device)
+        self.rows, self.cols = cm.rows, cm.cols
+        self.min_value, self.G = int(cm.min_value), int(len(cm.cdf) - 1)
+        self.payload_size = int(len(cm.payload))
+        pay = np.zeros(self.payload_size + 8, np.uint16)  # keep the tail 16-byte readable
+        pay[:self.payload_size] = cm.payload
+        self.payload = _dev(pay, self.device)
+        self.cursors = _dev(np.asarray(cm.cursors, np.uint32), self.device)
+        self.cdf = _dev(np.asarray(cm.cdf, np.uint8), self.device)
+        self.ppf = _dev(np.asarray(cm.ppf, np.uint8), self.device)
+
+    @classmethod
+    def encode(cls, W, device="cuda"):
+        from . import codec
+        return cls(codec.encode_matrix(W), device)
+
+    @property
+    def payload_bytes(self):
+        return 2 * self.payload_size + 4 * self.rows + 256 + self.G + 1
+
+    def _launch(self, x2, B, y, scales, ys):
+        check(lib().mv_wpr_matvec(_p(self.payload), self.payload_size, _p(self.cursors),
+                                  ctypes.c_int8(self.min_value), _p(self.cdf), self.G, _p(self.ppf), self.rows,
+                                  self.cols, _p(x2), B, _p(y), _p(scales), _p(ys), _stream()))
+
+
+class Q8Matrix(_Matrix):
+    """A matrix in this library's Q8-stripe layout (global or per-row tables)."""
+
+    def __init__(self, enc, device="cuda"):
+        self.device = torch.device(device)
+        self.rows, self.cols = int(enc["rows"]), int(enc["cols"])
+        self.blocks = _dev(enc["blocks"], self.device)
+        self.blk_off = _dev(enc["blk_off"], self.device)
+        self.tbl = _dev(np.asarray(enc["tbl"], np.uint16).view(np.int16), self.device)
+        self.tbl_off = _dev(enc["tbl_off"], self.device)
+        self.seg_quads, self.nseg = int(enc["seg_quads"]), int(enc["nseg"])
+        self.local, self.max_blk_rows = int(enc["local"]), int(enc["max_blk_rows"])
+        self.payload_bytes = int(enc["payload_bytes"])
+        self.bits_per_weight = float(enc["bits_per_weight"])
+        self._view = self.view()
+
+    @classmethod
+    def encode(cls, W, local=True, seg_quads=0, device="cuda"):
+        from . import codec
+        return cls(codec.q8_encode(W, local=local, seg_quads=seg_quads), device)
+
+    def view(self):
+        return Q8View(self.blocks.data_ptr(), self.blk_off.data_ptr(), self.tbl.data_ptr(),
+                      self.tbl_off.data_ptr(), self.rows, self.cols, self.seg_quads, self.nseg, self.local,
+                      self.max_blk_rows, self.blocks.numel() // 32, self.tbl.numel())
+
+    def _launch(self, x2, B, y, scales, ys):
+        check(lib().mv_q8_matvec(ctypes.byref(self._view), _p(x2), B, _p(y), _p(scales), _p(ys), _stream()))
+
+    def decode(self):
+        W = torch.empty((self.rows, self.cols), dtype=torch.int8, device=self.device)
+        check(lib().mv_q8_decode(ctypes.byref(self._view), _p(W), _stream()))
+        return W
+
+
+def dense_matvec(W, x, out=None):
+    """Dense int8 comparator y = W x on the GPU (W [rows, cols] int8 device tensor)."""
+    rows, cols = W.shape
+    x2, squeeze = _as_x(x, cols, W.device)
+    y = out if out is not None else torch.empty((x2.shape[0], rows), dtype=torch.int32, device=W.device)
+    check(lib().mv_dense_matvec(_p(W), rows, cols, _p(x2), x2.shape[0], _p(y), _stream()))
+    return y[0] if squeeze else y
+
+
+def mat_vec_mul_coalesced(in_vector_gpu, out_vector_gpu, in_dim, out_dim, scale, compressed, warp_offsets, ppf,
+                          ppf_cum, ppf_prob):
+    """The reference launcher of buffered/ans-warp-rows.cu:38-60, on torch device tensors
+    (legacy default stream, like the reference)."""
+    lib().mat_vec_mul_coalesced(_p(in_vector_gpu), _p(out_vector_gpu), int(in_dim), int(out_dim),
+                                ctypes.c_float(scale), _p(compressed), _p(warp_offsets), _p(ppf), _p(ppf_cum),
+                                _p(ppf_prob))
+    err = lib().mv_last_error().decode()
+    return err
+
+
+def requant_absmax(y, out8=None):
+    """Fused epilogue of matvansWarpPerRow.cu:51-72,167-172: returns (int8 vector, delta tensor)."""
+    n = y.numel()
+    out8 = out8 if out8 is not None else torch.empty(n, dtype=torch.int8, device=y.device)
+    delta = torch.empty(1, dtype=torch.float32, device=y.device)
+    scratch = torch.empty(1, dtype=torch.int32, device=y.device)
+    check(lib().mv_requant_absmax(_p(y), n, _p(out8), _p(delta), _p(scratch), _stream()))
+    return out8, delta
