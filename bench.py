@@ -264,6 +264,15 @@ def run_ours(args):
         for e in entries:
             e["M"].matvec(xd[e["cols"]][None], out=e["y"])
 
+    if args.profile:  # small fixed case for ncu: the gate above + two plain steps
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        ops.device_status()
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
@@ -307,6 +316,7 @@ def run_ours(args):
                                       "tbl": M.tbl.cpu().numpy().view(np.uint16),
                                       "tbl_off": M.tbl_off.cpu().numpy(), "seg_quads": M.seg_quads,
                                       "nseg": M.nseg, "local": M.local, "max_blk_rows": M.max_blk_rows,
+                                      "tbl_stripe_max": M.tbl_stripe_max,
                                       "payload_bytes": M.payload_bytes, "bits_per_weight": M.bits_per_weight},
                                      device=dev) for _ in range(R - 1)]
         x1 = xd[e["cols"]][None]
@@ -430,6 +440,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="run the correctness gate and two steps only (the case ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -146,6 +146,8 @@ typedef struct mv_q8_view {
     int32_t max_blk_rows;     /* max word-rows of any block                  */
     uint32_t blocks_rows;     /* word-rows (128 bytes) readable at `blocks`  */
     uint32_t tbl_len;         /* u16 entries readable at `tbl`               */
+    uint32_t tbl_stripe_max;  /* max entries of one stripe's 32 tables (local)
+                                 or of the global table                      */
 } mv_q8_view;
 
 /* y = W x for any batch >= 1 (passes of up to 16 vectors share one decode). */
@@ -194,7 +196,7 @@ mv_status mv_wpr_encode(const int8_t *W, int rows, int cols, int nthreads, mv_bl
 /* Q8-stripe encoder.  local = 1 fits one table per row, 0 one table for the
  * matrix.  seg_quads = 0 picks the segment length automatically.  Arrays:
  * "blocks" u32, "blk_off" u32, "tbl" u16, "tbl_off" u32; scalars "rows",
- * "cols", "seg_quads", "nseg", "local", "max_blk_rows", "payload_bytes"
+ * "cols", "seg_quads", "nseg", "local", "max_blk_rows", "tbl_stripe_max", "payload_bytes"
  * (blocks + tables + offsets). */
 mv_status mv_q8_encode(const int8_t *W, int rows, int cols, int local, int seg_quads,
                        int nthreads, mv_blob **out);

@@ -39,7 +39,7 @@ class Q8View(ctypes.Structure):
                 ("tbl_off", ctypes.c_void_p), ("rows", ctypes.c_int32), ("cols", ctypes.c_int32),
                 ("seg_quads", ctypes.c_int32), ("nseg", ctypes.c_int32), ("local", ctypes.c_int32),
                 ("max_blk_rows", ctypes.c_int32), ("blocks_rows", ctypes.c_uint32),
-                ("tbl_len", ctypes.c_uint32)]
+                ("tbl_len", ctypes.c_uint32), ("tbl_stripe_max", ctypes.c_uint32)]
 
 
 _LIB = None

@@ -315,7 +315,8 @@ def q8_encode(matrix, local=True, seg_quads=0, nthreads=0):
                              ctypes.byref(h)))
     b = Blob(h.value)
     out = {k: b.array(k) for k in ("blocks", "blk_off", "tbl", "tbl_off")}
-    for k in ("rows", "cols", "seg_quads", "nseg", "local", "max_blk_rows", "payload_bytes", "stream_bytes"):
+    for k in ("rows", "cols", "seg_quads", "nseg", "local", "max_blk_rows", "tbl_stripe_max", "payload_bytes",
+              "stream_bytes"):
         out[k] = b.scalar(k)
     out["bits_per_weight"] = 8.0 * out["payload_bytes"] / (out["rows"] * out["cols"])
     return out

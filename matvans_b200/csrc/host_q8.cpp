@@ -256,6 +256,13 @@ static mv_status q8_encode(const int8_t *W, int rows, int cols, int local, int s
         tbl.insert(tbl.end(), t.entries.begin(), t.entries.end());
     }
     tbl_off.push_back((uint32_t)tbl.size());
+    uint32_t stripe_max = 0;
+    if (e.local) {
+        for (int s = 0; s < e.stripes; s++)
+            stripe_max = std::max(stripe_max, tbl_off[(size_t)s * 32 + 32] - tbl_off[(size_t)s * 32]);
+    } else {
+        stripe_max = tbl_off[1] - tbl_off[0];
+    }
 
     const int64_t payload = (int64_t)total_rows * 128 + (int64_t)tbl.size() * 2 +
                             (int64_t)tbl_off.size() * 4 + (int64_t)blk_off.size() * 4;
@@ -273,6 +280,7 @@ static mv_status q8_encode(const int8_t *W, int rows, int cols, int local, int s
     out.set("nseg", e.nseg);
     out.set("local", e.local ? 1 : 0);
     out.set("max_blk_rows", max_rows);
+    out.set("tbl_stripe_max", stripe_max);
     out.set("payload_bytes", payload);
     out.set("stream_bytes", (int64_t)total_rows * 128);
     return MV_OK;

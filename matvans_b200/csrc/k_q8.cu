@@ -40,6 +40,7 @@ struct Q8Launch {
     int buf_words;         // per-warp buffer, u32 words (multiple of 32)
     int range_quads;       // quads staged per CTA (= W * seg_quads)
     int xs_words;          // staged x words, rounded to a multiple of 4
+    int tbl_stage;         // u16 table entries staged per CTA (multiple of 8)
     uint32_t spin_limit;   // barrier wait bound (iterations)
     int drop_copy;         // fault injection: do not issue the bulk copies
 };
@@ -65,6 +66,8 @@ __global__ void __launch_bounds__(512) q8_kernel(const Q8Launch L) {
     uint32_t *xs = bufs + W * L.buf_words;
     int *red = reinterpret_cast<int *>(xs + L.xs_words);
     uint64_t *bars = reinterpret_cast<uint64_t *>(red + (DECODE ? 0 : W * NV * 32));
+    uint32_t *toff_s = reinterpret_cast<uint32_t *>(bars + W);  // [33]
+    uint16_t *tsm = reinterpret_cast<uint16_t *>(toff_s + 36);  // [tbl_stage]
 
     const int stripe = blockIdx.x;
     const int seg = blockIdx.y * W + warp;
@@ -92,26 +95,20 @@ __global__ void __launch_bounds__(512) q8_kernel(const Q8Launch L) {
         blk_rows = __shfl_sync(0xffffffffu, blk_rows, 0);
     }
 
-    // (2) decode table: warp w fills quantiles [qlo, qhi) of all 32 rows
+    // (2a) stage this stripe's tables (local: 32 consecutive row tables; global: one)
     {
-        const int row_tbl = m.local ? stripe * 32 + lane : 0;
-        uint32_t t0 = __ldg(m.tbl_off + row_tbl), t1 = __ldg(m.tbl_off + row_tbl + 1);
-        if (t1 < t0 || t1 > m.tbl_len) t0 = t1 = 0;  // caught below as a short table
-        const int qlo = (256 * warp) / W, qhi = (256 * (warp + 1)) / W;
-        uint32_t cum = 0;
-        for (uint32_t k = t0; k < t1 && cum < (uint32_t)qhi; k++) {
-            const uint32_t ent = __ldg(m.tbl + k);
-            const uint32_t f = ent >> 8, sym = ent & 0xFF;
-            const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
-            for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = sym | (f << 8) | ((q - cum) << 16);
-            cum += f;
+        const uint32_t r0 = m.local ? (uint32_t)stripe * 32 : 0;
+        const uint32_t nt = m.local ? 32 : 1;
+        const uint32_t tb = __ldg(m.tbl_off + r0), te = __ldg(m.tbl_off + r0 + nt);
+        const bool ok = te >= tb && te <= m.tbl_len && te - tb <= (uint32_t)L.tbl_stage;
+        if (threadIdx.x <= nt) {
+            const uint32_t o = __ldg(m.tbl_off + r0 + threadIdx.x);
+            toff_s[threadIdx.x] = (ok && o >= tb && o <= te) ? o - tb : 0;
         }
-        if (cum < (uint32_t)qhi) {  // table sums to less than 256: fill and flag
-            for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) lut[q * 32 + lane] = 1u << 8;
-            atomicOr(L.status, MV_DEV_BAD_TABLE);
-        }
+        if (!ok && threadIdx.x == 0) atomicOr(L.status, MV_DEV_BAD_TABLE);
+        const uint32_t n = ok ? te - tb : 0;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) tsm[i] = __ldg(m.tbl + tb + i);
     }
-
     // (3) stage x quads of this CTA's column range
     if (!DECODE) {
         const int nquads = min(L.range_quads, qtot - qa);
@@ -121,6 +118,27 @@ __global__ void __launch_bounds__(512) q8_kernel(const Q8Launch L) {
             uint32_t val = 0;
             if (c < nquads && v < L.batch) val = load_x_quad(L.x + (size_t)v * m.cols, m.cols, qa + c, aligned);
             xs[i] = val;
+        }
+    }
+    __syncthreads();
+
+    // (2b) decode table: warp w fills quantiles [qlo, qhi) of all 32 rows from
+    // the staged entries; lane = row, so every store hits the lane's own bank
+    {
+        const int t = m.local ? lane : 0;
+        const uint32_t o0 = toff_s[t], o1 = max(toff_s[t + 1], o0);
+        const int qlo = (256 * warp) / W, qhi = (256 * (warp + 1)) / W;
+        uint32_t cum = 0;
+        for (uint32_t k = o0; k < o1 && cum < (uint32_t)qhi; k++) {
+            const uint32_t ent = tsm[k];
+            const uint32_t f = ent >> 8, sym = ent & 0xFF;
+            const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
+            for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = sym | (f << 8) | ((q - cum) << 16);
+            cum += f;
+        }
+        if (cum < (uint32_t)qhi) {  // table sums to less than 256: fill and flag
+            for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) lut[q * 32 + lane] = 1u << 8;
+            atomicOr(L.status, MV_DEV_BAD_TABLE);
         }
     }
     __syncthreads();
@@ -227,11 +245,13 @@ __global__ void scale_rows_kernel(const int32_t *y, const float *s, float *ys, i
 
 namespace {
 
+int tbl_stage_entries(const mv_q8_view &m) { return (int)((m.tbl_stripe_max + 7) & ~7u); }
+
 size_t q8_smem_bytes(const mv_q8_view &m, int W, int nv, bool decode) {
     const size_t range = (size_t)W * m.seg_quads;
     const size_t xs_words = decode ? 0 : ((range * nv + 3) & ~(size_t)3);
     return 256 * 32 * 4 + (size_t)W * (m.max_blk_rows + 1) * 32 * 4 + xs_words * 4 +
-           (decode ? 0 : (size_t)W * nv * 32 * 4) + (size_t)W * 8;
+           (decode ? 0 : (size_t)W * nv * 32 * 4) + (size_t)W * 8 + 36 * 4 + (size_t)tbl_stage_entries(m) * 2;
 }
 
 template <int NV, bool DECODE>
@@ -242,6 +262,7 @@ mv_status launch_q8(const Q8Launch &base, int W, int ngroups, cudaStream_t st) {
     const int nvw = NV > 0 ? NV : 0;
     L.xs_words = DECODE ? 0 : ((L.range_quads * nvw + 3) & ~3);
     L.buf_words = (m.max_blk_rows + 1) * 32;
+    L.tbl_stage = tbl_stage_entries(m);
     const size_t smem = q8_smem_bytes(m, W, nvw, DECODE);
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "Q8 launch needs %zu B of shared memory (max %d)", smem,
@@ -266,6 +287,8 @@ mv_status check_view(const mv_q8_view *m) {
         return fail(MV_ERR_ARG, "mv_q8: nseg * seg_quads does not cover the columns");
     if (((uintptr_t)m->blocks & 15) != 0) return fail(MV_ERR_ARG, "mv_q8: blocks not 16-byte aligned");
     if (m->blocks_rows < 2 || m->tbl_len < 2) return fail(MV_ERR_ARG, "mv_q8: empty blocks or tables");
+    if (m->tbl_stripe_max < 2 || m->tbl_stripe_max > 32 * 256)
+        return fail(MV_ERR_ARG, "mv_q8: tbl_stripe_max out of range");
     return MV_OK;
 }
 

@@ -158,6 +158,7 @@ class Q8Matrix(_Matrix):
         self.tbl_off = _dev(enc["tbl_off"], self.device)
         self.seg_quads, self.nseg = int(enc["seg_quads"]), int(enc["nseg"])
         self.local, self.max_blk_rows = int(enc["local"]), int(enc["max_blk_rows"])
+        self.tbl_stripe_max = int(enc["tbl_stripe_max"])
         self.payload_bytes = int(enc["payload_bytes"])
         self.bits_per_weight = float(enc["bits_per_weight"])
         self._view = self.view()
@@ -170,7 +171,7 @@ class Q8Matrix(_Matrix):
     def view(self):
         return Q8View(self.blocks.data_ptr(), self.blk_off.data_ptr(), self.tbl.data_ptr(),
                       self.tbl_off.data_ptr(), self.rows, self.cols, self.seg_quads, self.nseg, self.local,
-                      self.max_blk_rows, self.blocks.numel() // 32, self.tbl.numel())
+                      self.max_blk_rows, self.blocks.numel() // 32, self.tbl.numel(), self.tbl_stripe_max)
 
     def _launch(self, x2, B, y, scales, ys):
         check(lib().mv_q8_matvec(ctypes.byref(self._view), _p(x2), B, _p(y), _p(scales), _p(ys), _stream()))
