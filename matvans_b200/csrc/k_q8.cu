@@ -101,9 +101,9 @@ __global__ void __launch_bounds__(512) q8_kernel(const Q8Launch L) {
         const uint32_t nt = m.local ? 32 : 1;
         const uint32_t tb = __ldg(m.tbl_off + r0), te = __ldg(m.tbl_off + r0 + nt);
         const bool ok = te >= tb && te <= m.tbl_len && te - tb <= (uint32_t)L.tbl_stage;
-        if (threadIdx.x <= nt) {
-            const uint32_t o = __ldg(m.tbl_off + r0 + threadIdx.x);
-            toff_s[threadIdx.x] = (ok && o >= tb && o <= te) ? o - tb : 0;
+        for (uint32_t i = threadIdx.x; i <= nt; i += blockDim.x) {
+            const uint32_t o = __ldg(m.tbl_off + r0 + i);
+            toff_s[i] = (ok && o >= tb && o <= te) ? o - tb : 0;
         }
         if (!ok && threadIdx.x == 0) atomicOr(L.status, MV_DEV_BAD_TABLE);
         const uint32_t n = ok ? te - tb : 0;
