@@ -120,6 +120,21 @@ mv_status mv_wpr_matvec(const uint16_t *payload_dev, size_t payload_size,
 mv_status mv_requant_absmax(const int32_t *y_dev, int n, int8_t *out8_dev, float *delta_dev,
                             uint32_t *absmax_scratch_dev, void *stream);
 
+/* Allocation-free variant of mv_requant_absmax.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory: code enqueued
+ * during CUDA graph capture, plugins whose host framework owns the allocator,
+ * latency-critical paths that cannot afford cudaMalloc's implicit
+ * synchronisation.  Same inputs, outputs and results as mv_requant_absmax,
+ * but the reduction scratch is a 16 KiB array compiled into the library
+ * (held on every GPU that loads it, until exit), so it calls no allocating
+ * routine.  n <= 33,554,432, else MV_ERR_ARG.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture on that device.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised; no state needs
+ * clearing between calls. */
+mv_status mv_requant_absmax_noalloc(const int32_t *y_dev, int n, int8_t *out8_dev, float *delta_dev,
+                                    void *stream);
+
 /* ------------------------------------------------------------------- Q8 --- */
 
 /* Device view of one Q8-stripe matrix (all pointers are device pointers).

@@ -23,7 +23,7 @@ EXPORTS = [
     "mv_awr_matvec_requant", "mv_wpr_matvec", "mv_requant_absmax", "mv_q8_matvec", "mv_q8_decode",
     "mv_dense_matvec", "mv_blob_free", "mv_blob_get", "mv_blob_get_i64", "mv_blob_name", "mv_awr_encode",
     "mv_wpr_encode", "mv_q8_encode", "mv_read_safetensors", "mv_write_safetensors", "mv_read_wpr_bin",
-    "mv_hash_int8", "mv_debug_inject",
+    "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc",
 ]
 
 
@@ -63,6 +63,7 @@ def lib():
         "mv_awr_matvec_requant": ([P, sz, P, P, P, P, i32, i32, P, ctypes.c_float, P, P], st),
         "mv_wpr_matvec": ([P, sz, P, ctypes.c_int8, P, i32, P, i32, i32, P, i32, P, P, P, P], st),
         "mv_requant_absmax": ([P, i32, P, P, P, P], st),
+        "mv_requant_absmax_noalloc": ([P, i32, P, P, P], st),
         "mv_q8_matvec": ([ctypes.POINTER(Q8View), P, i32, P, P, P, P], st),
         "mv_q8_decode": ([ctypes.POINTER(Q8View), P, P], st),
         "mv_dense_matvec": ([P, i32, i32, P, i32, P, P], st),
