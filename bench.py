@@ -249,20 +249,25 @@ def run_ours(args):
             M = ops.Q8Matrix.encode(m["W"], local=local_cdf, device=dev)
             rows, cols = m["shape"]
             entries.append(dict(name=f"{rows}x{cols}_s{int(m['sigma'])}_{'local' if local_cdf else 'global'}",
-                                M=M, rows=rows, cols=cols, sigma=m["sigma"], entropy=H,
-                                y=torch.empty((1, rows), dtype=torch.int32, device=dev),
+                                M=M, rows=rows, cols=cols, sigma=m["sigma"], entropy=H, W=m["W"],
                                 alg_bytes=M.payload_bytes + cols + 4 * rows))
+    xs = [xd[e["cols"]][None].contiguous() for e in entries]
+
+    # one step = one persistent launch over all 12 matrices (mv_q8_stack_matvec)
+    from matvans_b200 import autotune
+    stack_tuning, stack_cands = autotune.tune_stack(
+        lambda t: ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=t, xs=xs, device=dev))
+    S = ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=stack_tuning, xs=xs, device=dev)
     # correctness gate before timing: bit-exact against the host int64 matvec
-    for e, m in zip(entries, [m for m in mats for _ in (0, 1)]):
-        y = e["M"].matvec(xd[e["cols"]][None], out=e["y"]).cpu().numpy()[0]
-        ref = (m["W"].astype(np.int32) @ x_by_cols[e["cols"]].astype(np.int32))
-        if not np.array_equal(y, ref):
+    S.run()
+    for e, y in zip(entries, S.ys):
+        ref = (e["W"].astype(np.int32) @ x_by_cols[e["cols"]].astype(np.int32))
+        if not np.array_equal(y.cpu().numpy()[0], ref):
             raise SystemExit(f"bench: {e['name']} is not bit-exact")
     ops.device_status()
 
     def step():
-        for e in entries:
-            e["M"].matvec(xd[e["cols"]][None], out=e["y"])
+        S.run()
 
     if args.profile:  # small fixed case for ncu: the gate above + two plain steps
         for _ in range(2):
@@ -310,21 +315,11 @@ def run_ours(args):
     per = {}
     for e in entries:
         M = e["M"]
-        R = copies_for(M.payload_bytes)
-        copies = [M] + [ops.Q8Matrix({"rows": M.rows, "cols": M.cols, "blocks": M.blocks.cpu().numpy(),
-                                      "blk_off": M.blk_off.cpu().numpy(),
-                                      "tbl": M.tbl.cpu().numpy().view(np.uint16),
-                                      "tbl_off": M.tbl_off.cpu().numpy(), "seg_quads": M.seg_quads,
-                                      "nseg": M.nseg, "local": M.local, "max_blk_rows": M.max_blk_rows,
-                                      "tbl_stripe_max": M.tbl_stripe_max,
-                                      "payload_bytes": M.payload_bytes, "bits_per_weight": M.bits_per_weight},
-                                     device=dev) for _ in range(R - 1)]
-        x1 = xd[e["cols"]][None]
-        t_ms, _ = time_graph(torch, lambda: [c.matvec(x1, out=e["y"]) for c in copies], 20, inner=R)
+        tun, info = autotune.tune(M, batch=1)
+        t_ms = info["us"] * 1e-3
         per[e["name"]] = {"us": 1e3 * t_ms, "int8_equiv_gbs": int8_equiv_bytes(e["rows"], e["cols"]) / t_ms / 1e6,
                           "compressed_gbs": e["alg_bytes"] / t_ms / 1e6, "bits_per_weight": M.bits_per_weight,
-                          "entropy_bits": e["entropy"]}
-        del copies
+                          "entropy_bits": e["entropy"], "tuning": [tun.warps, tun.ilp, tun.depth, tun.ctas_per_sm]}
     torch.cuda.empty_cache()
     dense, cublas, awr_t, wpr_t = {}, {}, {}, {}
     for m in mats:
@@ -371,13 +366,15 @@ def run_ours(args):
     xh = {c: torch.from_numpy(v).pin_memory() for c, v in x_by_cols.items()}
     yh = [torch.empty((1, e["rows"]), dtype=torch.int32).pin_memory() for e in entries]
     xin = {c: torch.empty((1, c), dtype=torch.int8, device=dev) for c in xh}
+    S_e2e = ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=stack_tuning,
+                        xs=[xin[e["cols"]] for e in entries], device=dev)
 
     def e2e_step():
         for c in xh:
             xin[c].copy_(xh[c][None], non_blocking=True)
-        for e, h in zip(entries, yh):
-            e["M"].matvec(xin[e["cols"]], out=e["y"])
-            h.copy_(e["y"], non_blocking=True)
+        S_e2e.run()
+        for y, h in zip(S_e2e.ys, yh):
+            h.copy_(y, non_blocking=True)
 
     for _ in range(3):
         e2e_step()
@@ -407,7 +404,9 @@ def run_ours(args):
                                    "per step, B=1, seeded synthetic int8 weights and x",
                        "batch": 1, "matvecs_per_step": len(entries), "seed": 20251203,
                        "l2": f"working set {alg / 2**20:.0f} MiB > 126 MiB L2, each matrix read once per step",
-                       "timing": "CUDA graph of one step, CUDA events over K replays, max over ranks"},
+                       "timing": "CUDA graph of one step (one persistent launch over the 12 matrices), CUDA "
+                                 "events over K replays, max over ranks",
+                       "stack_tuning": list(stack_tuning), "stack_candidates_us": stack_cands},
             "us_per_matvec": {k: round(v["us"], 3) for k, v in per.items()},
             "per_matrix": per,
             "dense_dp4a": dense, "cublas_sgemv_fp32": cublas, "ans_warp_rows_kernel": awr_t,
@@ -416,9 +415,9 @@ def run_ours(args):
                                       for k, v in per.items() if k.split("_s")[0] in dense and "_s4_" in k},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "q8_kernel<1,false>",
+                         "kernel": "q8s_kernel<1,ILP,DEPTH> (mv_q8_stack_matvec)",
                          "note": "algorithmic bytes = compressed streams + tables + offsets + x + int32 y"},
-            "gpu_launches": args.steps * len(entries),
+            "gpu_launches": args.steps * 3,
             "clocks": sampler.summary(),
             "e2e": {"value": world * step_bytes / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

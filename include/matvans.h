@@ -169,6 +169,60 @@ typedef struct mv_q8_view {
 mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int32_t *y_dev,
                        const float *row_scales_dev, float *y_scaled_dev, void *stream);
 
+/* Launch parameters of the persistent Q8 kernel (0 = library default).
+ *   warps        warps per CTA (1..8, default 8)
+ *   ilp          independent segments decoded per warp (1 or 2, default 2)
+ *   depth        shared-memory stream buffers per warp (1 or 2, default 1):
+ *                2 keeps the next work item's bulk copies in flight
+ *   ctas_per_sm  cap on resident CTAs per SM (default: occupancy limit) */
+typedef struct mv_q8_tuning {
+    int32_t warps, ilp, depth, ctas_per_sm;
+} mv_q8_tuning;
+
+/* mv_q8_matvec with explicit launch parameters (needs cols % 4 == 0 and a
+ * 4-byte aligned x; mv_q8_matvec itself falls back to a non-persistent kernel
+ * otherwise). */
+mv_status mv_q8_matvec_tuned(const mv_q8_view *m, const int8_t *x_dev, int batch, int32_t *y_dev,
+                             const float *row_scales_dev, float *y_scaled_dev,
+                             const mv_q8_tuning *tuning, void *stream);
+
+/* One matrix of a batched launch: the matrix, its input x [batch][cols] and
+ * outputs y [batch][rows] (+ optional scaled output).  ngroups, atomic and
+ * item0 are filled in by mv_q8_stack_plan. */
+typedef struct mv_q8_job {
+    mv_q8_view m;
+    const int8_t *x;
+    int32_t *y;
+    const float *scales;
+    float *ys;
+    int32_t ngroups;
+    int32_t atomic;
+    uint32_t item0;
+    uint32_t pad;
+} mv_q8_job;
+
+typedef struct mv_q8_stack_info {
+    uint32_t nitems;          /* work items (matrix, 32-row stripe, segment group) */
+    int32_t max_blk_rows;     /* shared-memory sizing over all jobs */
+    uint32_t tbl_stripe_max;
+    int32_t warps, ilp, depth;
+} mv_q8_stack_info;
+
+/* Plans a batched launch on the host: fills ngroups/atomic/item0 of every
+ * job for the given tuning and returns the sizes the launch needs.  The
+ * caller then copies `jobs` to device memory. */
+mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning,
+                           mv_q8_stack_info *info);
+
+/* Every job of a (device-resident, planned) job table in ONE persistent
+ * launch: CTAs walk the (matrix, stripe, segment-group) work items of all
+ * matrices, so uneven shapes share the GPU without per-matrix tails.  batch
+ * 1..16.  Launches three kernels (zero atomically-accumulated outputs, the
+ * persistent decode, scale them); capturable in a CUDA graph once the
+ * device status word exists (any earlier call creates it). */
+mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info,
+                             int batch, const mv_q8_tuning *tuning, void *stream);
+
 /* Decode the whole matrix to W_dev[rows][cols] (test / debugging aid). */
 mv_status mv_q8_decode(const mv_q8_view *m, int8_t *W_dev, void *stream);
 

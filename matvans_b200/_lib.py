@@ -23,7 +23,8 @@ EXPORTS = [
     "mv_awr_matvec_requant", "mv_wpr_matvec", "mv_requant_absmax", "mv_q8_matvec", "mv_q8_decode",
     "mv_dense_matvec", "mv_blob_free", "mv_blob_get", "mv_blob_get_i64", "mv_blob_name", "mv_awr_encode",
     "mv_wpr_encode", "mv_q8_encode", "mv_read_safetensors", "mv_write_safetensors", "mv_read_wpr_bin",
-    "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc",
+    "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc", "mv_q8_matvec_tuned", "mv_q8_stack_plan",
+    "mv_q8_stack_matvec",
 ]
 
 
@@ -40,6 +41,25 @@ class Q8View(ctypes.Structure):
                 ("seg_quads", ctypes.c_int32), ("nseg", ctypes.c_int32), ("local", ctypes.c_int32),
                 ("max_blk_rows", ctypes.c_int32), ("blocks_rows", ctypes.c_uint32),
                 ("tbl_len", ctypes.c_uint32), ("tbl_stripe_max", ctypes.c_uint32)]
+
+
+class Q8Tuning(ctypes.Structure):
+    """struct mv_q8_tuning."""
+    _fields_ = [("warps", ctypes.c_int32), ("ilp", ctypes.c_int32), ("depth", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32)]
+
+
+class Q8Job(ctypes.Structure):
+    """struct mv_q8_job."""
+    _fields_ = [("m", Q8View), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("scales", ctypes.c_void_p),
+                ("ys", ctypes.c_void_p), ("ngroups", ctypes.c_int32), ("atomic", ctypes.c_int32),
+                ("item0", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+
+class Q8StackInfo(ctypes.Structure):
+    """struct mv_q8_stack_info."""
+    _fields_ = [("nitems", ctypes.c_uint32), ("max_blk_rows", ctypes.c_int32), ("tbl_stripe_max", ctypes.c_uint32),
+                ("warps", ctypes.c_int32), ("ilp", ctypes.c_int32), ("depth", ctypes.c_int32)]
 
 
 _LIB = None
@@ -66,6 +86,9 @@ def lib():
         "mv_requant_absmax_noalloc": ([P, i32, P, P, P], st),
         "mv_q8_matvec": ([ctypes.POINTER(Q8View), P, i32, P, P, P, P], st),
         "mv_q8_decode": ([ctypes.POINTER(Q8View), P, P], st),
+        "mv_q8_matvec_tuned": ([ctypes.POINTER(Q8View), P, i32, P, P, P, ctypes.POINTER(Q8Tuning), P], st),
+        "mv_q8_stack_plan": ([ctypes.POINTER(Q8Job), i32, ctypes.POINTER(Q8Tuning), ctypes.POINTER(Q8StackInfo)], st),
+        "mv_q8_stack_matvec": ([P, i32, ctypes.POINTER(Q8StackInfo), i32, ctypes.POINTER(Q8Tuning), P], st),
         "mv_dense_matvec": ([P, i32, i32, P, i32, P, P], st),
         "mv_blob_free": ([P], None),
         "mv_blob_get": ([P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)], st),

@@ -1,0 +1,138 @@
+"""Per-shape launch-parameter autotuner for the persistent Q8 kernel, with a JSON cache.
+
+The tunables are the ones the kernel exposes through mv_q8_tuning: warps per
+CTA, independent streams decoded per warp (ilp) and shared-memory stream buffer
+depth (depth).  Stream interleave inside a row (segment length) is fixed when a
+matrix is encoded (q8_encode's seg_quads), so it is part of the cache key.
+
+Each candidate is timed as a CUDA graph of R launches over R copies of the
+matrix, enough copies that their compressed bytes exceed twice the L2, so every
+launch reads HBM as in real use.  The best candidate is cached under a key of
+GPU name, driver, library build, shape, table mode, segment length, bits per
+weight and batch, in $MATVANS_AUTOTUNE_CACHE (default
+~/.cache/matvans_b200/autotune.json).
+"""
+import json
+import os
+import threading
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import Q8Tuning
+
+CANDIDATES = [(w, ilp, d, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)]
+L2_BYTES = 126 * 2 ** 20
+_lock = threading.Lock()
+
+
+def cache_path():
+    return os.environ.get("MATVANS_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "matvans_b200", "autotune.json"))
+
+
+def _load():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(db):
+    p = cache_path()
+    os.makedirs(os.path.dirname(p), exist_ok=True)
+    tmp = p + f".tmp{os.getpid()}"
+    with open(tmp, "w") as f:
+        json.dump(db, f, indent=1, sort_keys=True)
+    os.replace(tmp, p)
+
+
+def _build_id():
+    st = os.stat(_lib.LIB_PATH)
+    return f"{st.st_size}-{int(st.st_mtime)}"
+
+
+def key(M, batch):
+    props = torch.cuda.get_device_properties(M.device)
+    drv = torch.cuda.get_device_capability(M.device)
+    return (f"{props.name}|sm{drv[0]}{drv[1]}|{_build_id()}|{M.rows}x{M.cols}|local{M.local}|seg{M.seg_quads}"
+            f"|bpw{M.bits_per_weight:.1f}|B{batch}")
+
+
+def _copies(M, n):
+    from .ops import Q8Matrix
+    enc = {"rows": M.rows, "cols": M.cols, "blocks": M.blocks.cpu().numpy(), "blk_off": M.blk_off.cpu().numpy(),
+           "tbl": M.tbl.cpu().numpy().view(np.uint16), "tbl_off": M.tbl_off.cpu().numpy(),
+           "seg_quads": M.seg_quads, "nseg": M.nseg, "local": M.local, "max_blk_rows": M.max_blk_rows,
+           "tbl_stripe_max": M.tbl_stripe_max, "payload_bytes": M.payload_bytes,
+           "bits_per_weight": M.bits_per_weight}
+    return [M] + [Q8Matrix(enc, device=M.device) for _ in range(n - 1)]
+
+
+def time_launches(fns, reps=10):
+    """ms per call of each fn in `fns`, replayed as one CUDA graph."""
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for f in fns:
+            f()
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for f in fns:
+            f()
+    g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps / len(fns)
+
+
+def tune(M, batch=1, candidates=CANDIDATES, reps=10, force=False):
+    """Best Q8Tuning for matrix M at `batch` vectors (cached)."""
+    k = key(M, batch)
+    with _lock:
+        db = _load()
+    if not force and k in db:
+        return Q8Tuning(*db[k]["tuning"]), db[k]
+    R = int(min(48, max(2, -(-2 * L2_BYTES // max(1, M.payload_bytes)))))
+    mats = _copies(M, R)
+    x = torch.randint(-127, 128, (batch, M.cols), dtype=torch.int8, device=M.device)
+    y = torch.empty((batch, M.rows), dtype=torch.int32, device=M.device)
+    results = {}
+    for cand in candidates:
+        t = Q8Tuning(*cand)
+        try:
+            ms = time_launches([lambda m=m, t=t: m.matvec(x, out=y, tuning=t) for m in mats], reps)
+        except _lib.MatvansError:
+            continue  # e.g. does not fit shared memory
+        results[",".join(map(str, cand))] = 1e3 * ms
+    if not results:
+        raise RuntimeError("autotune: no candidate launched")
+    best = min(results, key=results.get)
+    entry = {"tuning": [int(v) for v in best.split(",")], "us": results[best], "all": results, "copies": R}
+    with _lock:
+        db = _load()
+        db[k] = entry
+        _store(db)
+    return Q8Tuning(*entry["tuning"]), entry
+
+
+def tune_stack(make_stack, candidates=CANDIDATES, reps=10):
+    """Best tuning for a Q8Stack built by make_stack(tuning); returns (tuning, {cand: us per launch})."""
+    results = {}
+    for cand in candidates:
+        try:
+            S = make_stack(cand)
+            ms = time_launches([S.run], reps)
+        except _lib.MatvansError:
+            continue
+        results[",".join(map(str, cand))] = 1e3 * ms
+    best = min(results, key=results.get)
+    return tuple(int(v) for v in best.split(",")), results

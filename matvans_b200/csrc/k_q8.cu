@@ -303,12 +303,17 @@ int nv_for(int nb) { return nb <= 2 ? nb : nb <= 4 ? 4 : nb <= 8 ? 8 : 16; }
 
 }  // namespace
 
+bool q8s_supports(const mv_q8_view *m, const int8_t *x);
+mv_status q8s_matvec(const mv_q8_view *m, const int8_t *x, int batch, int32_t *y, const float *scales, float *ys,
+                     const mv_q8_tuning *tuning, cudaStream_t st);
+
 mv_status q8_matvec(const mv_q8_view *m, const int8_t *x, int batch, int32_t *y,
                     const float *scales, float *ys, cudaStream_t st) {
     mv_status rc = check_view(m);
     if (rc) return rc;
     if (!x || !y || batch <= 0) return fail(MV_ERR_ARG, "mv_q8_matvec: bad x/y/batch");
     if (ys && !scales) return fail(MV_ERR_ARG, "mv_q8_matvec: y_scaled needs row scales");
+    if (q8s_supports(m, x)) return q8s_matvec(m, x, batch, y, scales, ys, nullptr, st);
     uint32_t *status = device_status_word(&rc);
     if (rc) return rc;
     for (int v0 = 0; v0 < batch; v0 += 16) {

@@ -1,0 +1,544 @@
+// Persistent decode + int8 matvec over a list of Q8-stripe matrices
+// ("jobs": one matrix with its x and y each) in one launch, for sm_100a.
+//
+// Work item = (job, stripe, segment group).  A group is SG = W*ILP segments
+// of one stripe: warp w decodes segments g*SG + w (+ W) -- with ILP = 2 the
+// two segments are independent rANS streams interleaved in one instruction
+// stream, which hides the ~100-cycle latency chain of a decode step.  CTAs are
+// persistent and take items c, c + G, c + 2G, ... .
+//
+// Per item:
+//   * lane 0 of each warp moves the warp's stream blocks into shared memory
+//     with 1-D bulk copies (cp.async.bulk, TMA engine, no multicast) completing
+//     on an mbarrier; with DEPTH = 2 the copies of the CTA's next item are in
+//     flight while the current one is decoded;
+//   * the decode table (256 quantiles x 32 lanes, entry (q,l) at word q*32+l,
+//     conflict-free) is rebuilt only when the table changes: every item for
+//     per-row tables, once per job for a global table;
+//   * x is read through L1 with broadcast loads (all lanes of a warp read the
+//     same quad), so it needs no staging;
+//   * per-row partial sums are reduced across warps in shared memory and
+//     stored, or added with exact integer atomics when a row spans groups.
+//
+// Decode step (per lane, per quad of 4 symbols; table entry e = f | sym << 8
+// | r << 16 with f the symbol's frequency, r = q - cum):
+//   refill:   if (hi == 0) { hi = lo; lo = next word }
+//   lookups:  e_i = table[byte i of lo]
+//   update:   t2 = r2 + f2*r3, t1 = r1 + f1*t2 (dp2a: 16-bit x 8-bit dot
+//             products read f straight from the entry), t0 = r0 + f0*t1,
+//             P = (f0 f1)(f2 f3), (hi:lo) = hi*P + t0 (one 32x32->64 IMAD)
+#include <algorithm>
+#include <cstdio>
+
+#include "mv_device.cuh"
+
+namespace mv {
+
+typedef mv_q8_job Q8Job;
+
+__global__ void scale_rows_kernel(const int32_t *y, const float *s, float *ys, int rows, int batch, int ldy);
+
+struct Q8SLaunch {
+    Q8Job job0;            // the only job when jobs == nullptr
+    const Q8Job *jobs;     // device array of njobs jobs, or nullptr
+    int njobs;
+    uint32_t nitems;
+    int batch;           // valid vectors (<= NV)
+    int x_row_words;     // unused placeholder for alignment
+    uint32_t *status;
+    uint32_t spin_limit;
+    int drop_copy;
+    int buf_words;       // per segment buffer, u32 words
+    int tbl_stage;       // staged table entries
+    uint32_t lut_stride; // 32 (words per quantile row of the table); a runtime value on purpose
+};
+
+struct ItemInfo {
+    int job, stripe, group;
+};
+
+__device__ __forceinline__ const Q8Job &job_at(const Q8SLaunch &L, int j) { return L.jobs ? L.jobs[j] : L.job0; }
+
+__device__ __forceinline__ ItemInfo find_item(const Q8SLaunch &L, uint32_t it) {
+    if (!L.jobs) {
+        const int ng = L.job0.ngroups;
+        return ItemInfo{0, (int)(it / ng), (int)(it % ng)};
+    }
+    const Q8Job *jobs = L.jobs;
+    int lo = 0, hi = L.njobs - 1;
+    while (lo < hi) {  // last job with item0 <= it
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&jobs[mid].item0) <= it) lo = mid;
+        else hi = mid - 1;
+    }
+    const uint32_t rel = it - __ldg(&jobs[lo].item0);
+    const int ng = __ldg(&jobs[lo].ngroups);
+    return ItemInfo{lo, (int)(rel / ng), (int)(rel % ng)};
+}
+
+// Issue the bulk copies of one warp's segment(s) of an item (lane 0 only).
+template <int ILP>
+__device__ __forceinline__ void issue_item_copies(const Q8SLaunch &L, const Q8Job &J, const ItemInfo &I, int warp,
+                                                  int W, uint32_t *slot_bufs, uint64_t *bar, uint32_t *blk_rows) {
+    const mv_q8_view &m = J.m;
+    uint32_t total = 0;
+    uint32_t o0s[ILP], rows[ILP];
+#pragma unroll
+    for (int k = 0; k < ILP; k++) {
+        const int seg = I.group * W * ILP + k * W + warp;
+        rows[k] = 0;
+        o0s[k] = 0;
+        if (seg < m.nseg) {
+            const int b = I.stripe * m.nseg + seg;
+            const uint32_t o0 = __ldg(m.blk_off + b), o1 = __ldg(m.blk_off + b + 1);
+            const uint32_t r = o1 - o0;
+            if (o1 < o0 || o1 > m.blocks_rows || r < 2 || (int)r + 1 > L.buf_words / 32) {
+                atomicOr(L.status, MV_DEV_STREAM_OVERRUN);
+            } else {
+                rows[k] = r;
+                o0s[k] = o0;
+                total += r * 128u;
+            }
+        }
+        blk_rows[k] = rows[k];
+    }
+    mbar_arrive_expect_tx(bar, total);
+    if (!L.drop_copy) {
+#pragma unroll
+        for (int k = 0; k < ILP; k++)
+            if (rows[k]) bulk_g2s(slot_bufs + k * L.buf_words, m.blocks + (size_t)o0s[k] * 32, rows[k] * 128u, bar);
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ void load_x(const int8_t *x, int cols, int q, uint32_t (&xv)[NV]) {
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+        xv[v] = __ldg(reinterpret_cast<const uint32_t *>(x + (size_t)v * cols) + q);
+}
+
+// One decode step of one stream; returns the packed four symbols.
+__device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t &kidx, const uint32_t kend,
+                                            const uint32_t *buf, const uint32_t *lut_l, uint32_t stride,
+                                            uint32_t &P) {
+    const uint32_t w = buf[kidx];
+    if (hi == 0) {
+        hi = lo;
+        lo = w;
+        kidx = min(kidx + 32, kend);
+    }
+    const uint32_t a0 = __byte_perm(lo, 0, 0x4440), a1 = __byte_perm(lo, 0, 0x4441);
+    const uint32_t a2 = __byte_perm(lo, 0, 0x4442), a3 = __byte_perm(lo, 0, 0x4443);
+    // stride is 32 words, passed at run time so the index math stays an IMAD
+    const uint32_t e0 = lut_l[a0 * stride], e1 = lut_l[a1 * stride];
+    const uint32_t e2 = lut_l[a2 * stride], e3 = lut_l[a3 * stride];
+    const uint32_t r0 = __umulhi(e0, 65536u), r1 = __umulhi(e1, 65536u);
+    const uint32_t r2 = e2 >> 16, r3 = e3 >> 16;
+    const uint32_t t2 = __dp2a_lo(r3, e2, r2);      // r2 + f2*r3
+    const uint32_t t1 = __dp2a_lo(t2, e1, r1);      // r1 + f1*t2  (t2 < 2^16)
+    const uint32_t f1 = e1 & 0xFF, f3 = e3 & 0xFF;
+    const uint32_t p01 = __dp2a_lo(f1, e0, 0u);     // f0*f1
+    const uint32_t p23 = __dp2a_lo(f3, e2, 0u);     // f2*f3
+    const uint32_t f0 = e0 & 0xFF;
+    P = p01 * p23;
+    const uint32_t t0 = r0 + f0 * t1;
+    const unsigned long long s = (unsigned long long)hi * P + t0;
+    lo = (uint32_t)s;
+    hi = (uint32_t)(s >> 32);
+    return __byte_perm(__byte_perm(e0, e1, 0x0051), __byte_perm(e2, e3, 0x0051), 0x5410);
+}
+
+template <int NV, int ILP, int DEPTH>
+__global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int W = blockDim.x >> 5;
+
+    uint32_t *lut = reinterpret_cast<uint32_t *>(smem);                      // 8192 words
+    uint32_t *bufs = lut + 256 * 32;                                          // [W][DEPTH][ILP][buf_words]
+    int *red = reinterpret_cast<int *>(bufs + (size_t)W * DEPTH * ILP * L.buf_words);  // [W][NV][32]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(red + W * NV * 32);         // [W][DEPTH]
+    uint32_t *toff_s = reinterpret_cast<uint32_t *>(bars + W * DEPTH);        // [36]
+    uint32_t *rows_s = toff_s + 36;                                           // [W][DEPTH][ILP]
+    uint16_t *tsm = reinterpret_cast<uint16_t *>(rows_s + W * DEPTH * ILP);  // [tbl_stage]
+    uint32_t *my_rows = rows_s + warp * DEPTH * ILP;
+
+    uint32_t *my_bufs = bufs + (size_t)warp * DEPTH * ILP * L.buf_words;
+    if (lane == 0)
+        for (int d = 0; d < DEPTH; d++) mbar_init(&bars[warp * DEPTH + d], 1);
+    fence_mbar_init();
+    __syncwarp();
+
+    const uint32_t G = gridDim.x;
+    // prologue: copies of the first item (and the second with DEPTH = 2)
+    for (int d = 0; d < DEPTH; d++) {
+        const uint32_t it = blockIdx.x + d * G;
+        if (lane == 0) {
+            for (int k = 0; k < ILP; k++) my_rows[d * ILP + k] = 0;
+            if (it < L.nitems) {
+                const ItemInfo I = find_item(L, it);
+                issue_item_copies<ILP>(L, job_at(L, I.job), I, warp, W, my_bufs + d * ILP * L.buf_words,
+                                       &bars[warp * DEPTH + d], my_rows + d * ILP);
+            }
+        }
+    }
+    __syncwarp();
+
+    int lut_job = -1, lut_stripe = -1;
+    uint32_t iter = 0;
+    const uint32_t *lut_l = lut + lane;
+    for (uint32_t it = blockIdx.x; it < L.nitems; it += G, iter++) {
+        const int slot = DEPTH == 2 ? (int)(iter & 1) : 0;
+        const uint32_t parity = DEPTH == 2 ? ((iter >> 1) & 1) : (iter & 1);
+        const ItemInfo I = find_item(L, it);
+        const Q8Job &J = job_at(L, I.job);
+        const mv_q8_view &m = J.m;
+        uint32_t rows_now[ILP];
+#pragma unroll
+        for (int k = 0; k < ILP; k++) rows_now[k] = my_rows[slot * ILP + k];
+
+        // decode table (uniform decision across the CTA)
+        if (I.job != lut_job || (m.local && I.stripe != lut_stripe)) {
+            __syncthreads();  // every warp is done with the previous table
+            const uint32_t r0 = m.local ? (uint32_t)I.stripe * 32 : 0;
+            const uint32_t nt = m.local ? 32 : 1;
+            const uint32_t tb = __ldg(m.tbl_off + r0), te = __ldg(m.tbl_off + r0 + nt);
+            const bool ok = te >= tb && te <= m.tbl_len && te - tb <= (uint32_t)L.tbl_stage;
+            for (uint32_t i = threadIdx.x; i <= nt; i += blockDim.x) {
+                const uint32_t o = __ldg(m.tbl_off + r0 + i);
+                toff_s[i] = (ok && o >= tb && o <= te) ? o - tb : 0;
+            }
+            if (!ok && threadIdx.x == 0) atomicOr(L.status, MV_DEV_BAD_TABLE);
+            const uint32_t n = ok ? te - tb : 0;
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) tsm[i] = __ldg(m.tbl + tb + i);
+            __syncthreads();
+            const int t = m.local ? lane : 0;
+            const uint32_t o0 = toff_s[t], o1 = max(toff_s[t + 1], o0);
+            const int qlo = (256 * warp) / W, qhi = (256 * (warp + 1)) / W;
+            uint32_t cum = 0;
+            for (uint32_t k = o0; k < o1 && cum < (uint32_t)qhi; k++) {
+                const uint32_t ent = tsm[k];
+                const uint32_t f = ent >> 8, sym = ent & 0xFF;
+                const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
+                for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 8) | ((q - cum) << 16);
+                cum += f;
+            }
+            if (cum < (uint32_t)qhi) {
+                for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) lut[q * 32 + lane] = 1u;
+                atomicOr(L.status, MV_DEV_BAD_TABLE);
+            }
+            __syncthreads();
+            lut_job = I.job;
+            lut_stripe = I.stripe;
+        }
+
+        int acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = 0;
+        const int qtot = (m.cols + 3) >> 2;
+        uint32_t *sb = my_bufs + slot * ILP * L.buf_words;
+        bool have_any = false;
+#pragma unroll
+        for (int k = 0; k < ILP; k++) have_any |= rows_now[k] != 0;
+        if (have_any) {
+            if (!mbar_wait_bounded(&bars[warp * DEPTH + slot], parity, L.status, L.spin_limit)) {
+                mbar_wait_bounded(&bars[warp * DEPTH + slot], parity, nullptr, L.spin_limit);
+            } else {
+                const int segA = I.group * W * ILP + warp;
+                const int q0A = segA * m.seg_quads;
+                const int nqA = rows_now[0] ? min(m.seg_quads, qtot - q0A) : 0;
+                uint32_t loA = sb[lane], hiA = sb[32 + lane], kA = 64 + lane, PA = 0;
+                const uint32_t kendA = rows_now[0] * 32 + lane;
+                const int8_t *x = J.x;
+                if (ILP == 2) {
+                    uint32_t *sbB = sb + L.buf_words;
+                    const int segB = segA + W;
+                    const int q0B = segB * m.seg_quads;
+                    const int nqB = rows_now[ILP - 1] ? min(m.seg_quads, qtot - q0B) : 0;
+                    uint32_t loB = sbB[lane], hiB = sbB[32 + lane], kB = 64 + lane, PB = 0;
+                    const uint32_t kendB = rows_now[ILP - 1] * 32 + lane;
+                    const int nboth = min(nqA, nqB);
+                    int i = 0;
+#pragma unroll 2
+                    for (; i < nboth; i++) {
+                        uint32_t xa[NV], xb[NV];
+                        load_x<NV>(x, m.cols, q0A + i, xa);
+                        load_x<NV>(x, m.cols, q0B + i, xb);
+                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+                        const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) {
+                            acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
+                            acc[v] = __dp4a((int)wb, (int)xb[v], acc[v]);
+                        }
+                    }
+                    for (int j = i; j < nqA; j++) {
+                        uint32_t xa[NV];
+                        load_x<NV>(x, m.cols, q0A + j, xa);
+                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
+                    }
+                    for (int j = i; j < nqB; j++) {
+                        uint32_t xb[NV];
+                        load_x<NV>(x, m.cols, q0B + j, xb);
+                        const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wb, (int)xb[v], acc[v]);
+                    }
+                    if (nqB > 0 && (hiB != 0 || loB != PB)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+                } else {
+#pragma unroll 4
+                    for (int i = 0; i < nqA; i++) {
+                        uint32_t xa[NV];
+                        load_x<NV>(x, m.cols, q0A + i, xa);
+                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
+                    }
+                }
+                if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+            }
+        }
+        __syncwarp();
+        // this warp's slot is free again: start the copies of the item that will use it
+        if (lane == 0) {
+            const uint32_t nx = it + DEPTH * G;
+            for (int k = 0; k < ILP; k++) my_rows[slot * ILP + k] = 0;
+            if (nx < L.nitems) {
+                const ItemInfo N = find_item(L, nx);
+                issue_item_copies<ILP>(L, job_at(L, N.job), N, warp, W, sb, &bars[warp * DEPTH + slot],
+                                       my_rows + slot * ILP);
+            }
+        }
+        __syncwarp();
+
+        // reduce the W partials of each row of the stripe
+#pragma unroll
+        for (int v = 0; v < NV; v++) red[(warp * NV + v) * 32 + lane] = acc[v];
+        __syncthreads();
+        for (int t = threadIdx.x; t < NV * 32; t += blockDim.x) {
+            const int v = t >> 5, l = t & 31;
+            int sum = 0;
+            for (int w = 0; w < W; w++) sum += red[(w * NV + v) * 32 + l];
+            const int row = I.stripe * 32 + l;
+            if (row < m.rows && v < L.batch) {
+                int32_t *dst = J.y + (size_t)v * m.rows + row;
+                if (J.atomic) {
+                    atomicAdd(dst, sum);
+                } else {
+                    *dst = sum;
+                    if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
+                }
+            }
+        }
+        __syncthreads();  // red is reused by the next item
+    }
+}
+
+}  // namespace mv
+
+namespace mv {
+
+__global__ void q8s_zero_atomic_y(const Q8Job *jobs, int njobs, int batch) {
+    for (int j = blockIdx.y; j < njobs; j += gridDim.y) {
+        const Q8Job &J = jobs[j];
+        if (!J.atomic) continue;
+        const size_t n = (size_t)batch * J.m.rows;
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+            J.y[i] = 0;
+    }
+}
+
+__global__ void q8s_scale_atomic_y(const Q8Job *jobs, int njobs, int batch) {
+    for (int j = blockIdx.y; j < njobs; j += gridDim.y) {
+        const Q8Job &J = jobs[j];
+        if (!J.atomic || !J.ys) continue;
+        const size_t n = (size_t)batch * J.m.rows;
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+            J.ys[i] = (float)J.y[i] * J.scales[i % J.m.rows];
+    }
+}
+
+namespace {
+
+size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage) {
+    return 256 * 32 * 4 + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 + (size_t)W * DEPTH * 8 +
+           36 * 4 + (size_t)W * DEPTH * ILP * 4 + (size_t)tbl_stage * 2;
+}
+
+template <int NV, int ILP, int DEPTH>
+mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t st) {
+    const size_t smem = q8s_smem(NV, ILP, DEPTH, W, L.buf_words, L.tbl_stage);
+    if (smem > (size_t)max_smem_optin())
+        return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch needs %zu B of shared memory (max %d)", smem,
+                    max_smem_optin());
+    auto kern = q8s_kernel<NV, ILP, DEPTH>;
+    int bps = 0;
+    mv_status rc = prepare_kernel((const void *)kern, smem, 32 * W, &bps);
+    if (rc) return rc;
+    if (ctas_per_sm > 0) bps = std::min(bps, ctas_per_sm);
+    const long long grid = std::max(1LL, std::min<long long>(L.nitems, (long long)bps * sm_count()));
+    kern<<<(unsigned)grid, 32 * W, smem, st>>>(L);
+    MV_CUDA_TRY(cudaGetLastError(), "q8 stack kernel launch");
+    return MV_OK;
+}
+
+template <int NV>
+mv_status launch_q8s_nv(const Q8SLaunch &L, const mv_q8_tuning &t, cudaStream_t st) {
+    if (t.ilp == 2) {
+        if (t.depth == 2) return launch_q8s_t<NV, 2, 2>(L, t.warps, t.ctas_per_sm, st);
+        return launch_q8s_t<NV, 2, 1>(L, t.warps, t.ctas_per_sm, st);
+    }
+    if (t.depth == 2) return launch_q8s_t<NV, 1, 2>(L, t.warps, t.ctas_per_sm, st);
+    return launch_q8s_t<NV, 1, 1>(L, t.warps, t.ctas_per_sm, st);
+}
+
+mv_status launch_q8s(const Q8SLaunch &L, int nv, const mv_q8_tuning &t, cudaStream_t st) {
+    switch (nv) {
+        case 1: return launch_q8s_nv<1>(L, t, st);
+        case 2: return launch_q8s_nv<2>(L, t, st);
+        case 4: return launch_q8s_nv<4>(L, t, st);
+        case 8: return launch_q8s_nv<8>(L, t, st);
+        default: return launch_q8s_nv<16>(L, t, st);
+    }
+}
+
+int nv_round(int nb) { return nb <= 2 ? nb : nb <= 4 ? 4 : nb <= 8 ? 8 : 16; }
+
+mv_q8_tuning resolve(const mv_q8_tuning *t) {
+    mv_q8_tuning r{8, 2, 1, 0};
+    if (t) {
+        if (t->warps > 0) r.warps = std::min(8, t->warps);
+        if (t->ilp == 1 || t->ilp == 2) r.ilp = t->ilp;
+        if (t->depth == 1 || t->depth == 2) r.depth = t->depth;
+        if (t->ctas_per_sm > 0) r.ctas_per_sm = t->ctas_per_sm;
+    }
+    return r;
+}
+
+void plan_job(Q8Job &J, const mv_q8_tuning &t, uint32_t &item) {
+    const int sg = t.warps * t.ilp;
+    J.ngroups = (J.m.nseg + sg - 1) / sg;
+    J.atomic = J.ngroups > 1;
+    J.item0 = item;
+    item += (uint32_t)((J.m.rows + 31) / 32) * (uint32_t)J.ngroups;
+}
+
+}  // namespace
+
+bool q8s_supports(const mv_q8_view *m, const int8_t *x) {
+    return (m->cols & 3) == 0 && ((uintptr_t)x & 3) == 0;
+}
+
+// Single matrix through the persistent kernel (one inline job).
+mv_status q8s_matvec(const mv_q8_view *m, const int8_t *x, int batch, int32_t *y, const float *scales, float *ys,
+                     const mv_q8_tuning *tuning, cudaStream_t st) {
+    mv_status rc;
+    uint32_t *status = device_status_word(&rc);
+    if (rc) return rc;
+    const mv_q8_tuning t = resolve(tuning);
+    for (int v0 = 0; v0 < batch; v0 += 16) {
+        const int nb = std::min(16, batch - v0);
+        Q8SLaunch L{};
+        L.job0.m = *m;
+        L.job0.x = x + (size_t)v0 * m->cols;
+        L.job0.y = y + (size_t)v0 * m->rows;
+        L.job0.scales = scales;
+        L.job0.ys = ys ? ys + (size_t)v0 * m->rows : nullptr;
+        uint32_t items = 0;
+        plan_job(L.job0, t, items);
+        if (L.job0.atomic) L.job0.ys = nullptr;
+        L.jobs = nullptr;
+        L.njobs = 1;
+        L.nitems = items;
+        L.batch = nb;
+        L.status = status;
+        L.spin_limit = wait_spin_limit();
+        L.drop_copy = inject_drop_copy();
+        L.buf_words = (m->max_blk_rows + 1) * 32;
+        L.tbl_stage = (int)((m->tbl_stripe_max + 7) & ~7u);
+        L.lut_stride = 32;
+        if (L.job0.atomic)
+            MV_CUDA_TRY(cudaMemsetAsync(L.job0.y, 0, sizeof(int32_t) * (size_t)nb * m->rows, st), "cudaMemsetAsync(y)");
+        rc = launch_q8s(L, nv_round(nb), t, st);
+        if (rc) return rc;
+        if (ys && L.job0.atomic) {
+            const int n = nb * m->rows;
+            scale_rows_kernel<<<(n + 255) / 256, 256, 0, st>>>(L.job0.y, scales, ys + (size_t)v0 * m->rows, m->rows,
+                                                               nb, m->rows);
+            MV_CUDA_TRY(cudaGetLastError(), "scale_rows_kernel launch");
+        }
+    }
+    return MV_OK;
+}
+
+}  // namespace mv
+
+extern "C" {
+
+mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning, mv_q8_stack_info *info) {
+    if (!jobs || njobs <= 0 || !info) return mv::fail(MV_ERR_ARG, "mv_q8_stack_plan: bad arguments");
+    const mv_q8_tuning t = mv::resolve(tuning);
+    uint32_t item = 0;
+    info->max_blk_rows = 2;
+    info->tbl_stripe_max = 2;
+    for (int j = 0; j < njobs; j++) {
+        const mv_q8_view &m = jobs[j].m;
+        if (m.rows <= 0 || m.cols <= 0 || (m.cols & 3) || m.nseg <= 0 || m.seg_quads <= 0)
+            return mv::fail(MV_ERR_ARG, "mv_q8_stack_plan: job %d has a bad view (cols %% 4 must be 0)", j);
+        if ((uint64_t)item + (uint64_t)((m.rows + 31) / 32) * (uint64_t)m.nseg > 0xFFFFFFFFull)
+            return mv::fail(MV_ERR_SHAPE, "mv_q8_stack_plan: too many work items");
+        mv::plan_job(jobs[j], t, item);
+        info->max_blk_rows = std::max(info->max_blk_rows, m.max_blk_rows);
+        info->tbl_stripe_max = std::max(info->tbl_stripe_max, m.tbl_stripe_max);
+    }
+    info->nitems = item;
+    info->warps = t.warps;
+    info->ilp = t.ilp;
+    info->depth = t.depth;
+    return MV_OK;
+}
+
+mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info, int batch,
+                             const mv_q8_tuning *tuning, void *stream) {
+    if (!jobs_dev || njobs <= 0 || !info || batch <= 0 || batch > 16)
+        return mv::fail(MV_ERR_ARG, "mv_q8_stack_matvec: bad arguments (batch must be 1..16)");
+    const mv_q8_tuning t = mv::resolve(tuning);
+    if (t.warps != info->warps || t.ilp != info->ilp)
+        return mv::fail(MV_ERR_ARG, "mv_q8_stack_matvec: tuning differs from the one the jobs were planned with");
+    cudaStream_t st = (cudaStream_t)stream;
+    mv_status rc;
+    mv::Q8SLaunch L{};
+    L.status = mv::device_status_word(&rc);
+    if (rc) return rc;
+    L.jobs = jobs_dev;
+    L.njobs = njobs;
+    L.nitems = info->nitems;
+    L.batch = batch;
+    L.spin_limit = mv::wait_spin_limit();
+    L.drop_copy = mv::inject_drop_copy();
+    L.buf_words = (info->max_blk_rows + 1) * 32;
+    L.tbl_stage = (int)((info->tbl_stripe_max + 7) & ~7u);
+    L.lut_stride = 32;
+    dim3 zg(64, std::min(njobs, 1024));
+    mv::q8s_zero_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
+    MV_CUDA_TRY(cudaGetLastError(), "q8s_zero_atomic_y launch");
+    rc = mv::launch_q8s(L, mv::nv_round(batch), t, st);
+    if (rc) return rc;
+    mv::q8s_scale_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
+    MV_CUDA_TRY(cudaGetLastError(), "q8s_scale_atomic_y launch");
+    return MV_OK;
+}
+
+mv_status mv_q8_matvec_tuned(const mv_q8_view *m, const int8_t *x_dev, int batch, int32_t *y_dev,
+                             const float *row_scales_dev, float *y_scaled_dev, const mv_q8_tuning *tuning,
+                             void *stream) {
+    if (!m || !x_dev || !y_dev || batch <= 0) return mv::fail(MV_ERR_ARG, "mv_q8_matvec_tuned: bad arguments");
+    if (y_scaled_dev && !row_scales_dev) return mv::fail(MV_ERR_ARG, "mv_q8_matvec_tuned: y_scaled needs scales");
+    if (!mv::q8s_supports(m, x_dev))
+        return mv::fail(MV_ERR_ARG, "mv_q8_matvec_tuned: needs cols %% 4 == 0 and 4-byte aligned x");
+    return mv::q8s_matvec(m, x_dev, batch, y_dev, row_scales_dev, y_scaled_dev, tuning, (cudaStream_t)stream);
+}
+
+}  // extern "C"

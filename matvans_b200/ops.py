@@ -11,7 +11,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import Q8View, check, lib
+from ._lib import Q8Job, Q8StackInfo, Q8Tuning, Q8View, check, lib
 
 _STATUS_BITS = {1: "stream overrun", 2: "final coder state mismatch", 4: "wait timeout", 8: "bad table"}
 
@@ -60,7 +60,7 @@ class _Matrix:
     rows: int
     cols: int
 
-    def matvec(self, x, scales=None, out=None, out_scaled=None):
+    def matvec(self, x, scales=None, out=None, out_scaled=None, tuning=None):
         x2, squeeze = _as_x(x, self.cols, self.device)
         B = x2.shape[0]
         y = out if out is not None else torch.empty((B, self.rows), dtype=torch.int32, device=self.device)
@@ -70,7 +70,10 @@ class _Matrix:
             scales = scales.to(self.device, torch.float32).contiguous()
             ys = out_scaled if out_scaled is not None else torch.empty((B, self.rows), dtype=torch.float32,
                                                                       device=self.device)
-        self._launch(x2, B, y, scales, ys)
+        if tuning is not None:
+            self._launch_tuned(x2, B, y, scales, ys, tuning)
+        else:
+            self._launch(x2, B, y, scales, ys)
         if squeeze:
             return (y[0], ys[0]) if ys is not None else y[0]
         return (y, ys) if ys is not None else y
@@ -176,10 +179,62 @@ class Q8Matrix(_Matrix):
     def _launch(self, x2, B, y, scales, ys):
         check(lib().mv_q8_matvec(ctypes.byref(self._view), _p(x2), B, _p(y), _p(scales), _p(ys), _stream()))
 
+    def _launch_tuned(self, x2, B, y, scales, ys, tuning):
+        t = tuning if isinstance(tuning, Q8Tuning) else Q8Tuning(*tuning)
+        check(lib().mv_q8_matvec_tuned(ctypes.byref(self._view), _p(x2), B, _p(y), _p(scales), _p(ys),
+                                       ctypes.byref(t), _stream()))
+
     def decode(self):
         W = torch.empty((self.rows, self.cols), dtype=torch.int8, device=self.device)
         check(lib().mv_q8_decode(ctypes.byref(self._view), _p(W), _stream()))
         return W
+
+
+class Q8Stack:
+    """Many Q8 matrices (uneven shapes) with their inputs and outputs, run by ONE
+    persistent launch (mv_q8_stack_matvec).  Inputs x_i [batch, cols_i] and
+    outputs y_i [batch, rows_i] are fixed device tensors, so run() can be
+    captured in a CUDA graph and replayed."""
+
+    def __init__(self, matrices, batch=1, tuning=None, xs=None, scales=None, device="cuda"):
+        self.device = torch.device(device)
+        self.matrices = list(matrices)
+        self.batch = int(batch)
+        if not 1 <= self.batch <= 16:
+            raise ValueError("batch must be 1..16")
+        self.tuning = tuning if isinstance(tuning, Q8Tuning) else Q8Tuning(*(tuning or (0, 0, 0, 0)))
+        self.xs = xs if xs is not None else [torch.zeros((self.batch, M.cols), dtype=torch.int8, device=self.device)
+                                             for M in self.matrices]
+        self.ys = [torch.empty((self.batch, M.rows), dtype=torch.int32, device=self.device) for M in self.matrices]
+        self.scales = scales
+        self.yss = [torch.empty((self.batch, M.rows), dtype=torch.float32, device=self.device)
+                    for M in self.matrices] if scales is not None else None
+        n = len(self.matrices)
+        jobs = (Q8Job * n)()
+        for i, M in enumerate(self.matrices):
+            x = self.xs[i]
+            if x.dtype != torch.int8 or tuple(x.shape) != (self.batch, M.cols) or not x.is_contiguous():
+                raise ValueError(f"x[{i}] must be a contiguous int8 tensor of shape {(self.batch, M.cols)}")
+            jobs[i].m = M.view()
+            jobs[i].x = x.data_ptr()
+            jobs[i].y = self.ys[i].data_ptr()
+            if scales is not None:
+                jobs[i].scales = scales[i].data_ptr()
+                jobs[i].ys = self.yss[i].data_ptr()
+        self.info = Q8StackInfo()
+        check(lib().mv_q8_stack_plan(jobs, n, ctypes.byref(self.tuning), ctypes.byref(self.info)))
+        raw = np.frombuffer(bytes(jobs), dtype=np.uint8)
+        self.jobs_dev = torch.from_numpy(raw.copy()).to(self.device)
+        self._jobs_host = jobs
+
+    @property
+    def nitems(self):
+        return self.info.nitems
+
+    def run(self):
+        check(lib().mv_q8_stack_matvec(_p(self.jobs_dev), len(self.matrices), ctypes.byref(self.info), self.batch,
+                                       ctypes.byref(self.tuning), _stream()))
+        return self.ys
 
 
 def dense_matvec(W, x, out=None):
