@@ -255,8 +255,11 @@ def run_ours(args):
 
     # one step = one persistent launch over all 12 matrices (mv_q8_stack_matvec)
     from matvans_b200 import autotune
-    stack_tuning, stack_cands = autotune.tune_stack(
-        lambda t: ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=t, xs=xs, device=dev))
+    if args.tuning:
+        stack_tuning, stack_cands = tuple(int(v) for v in args.tuning.split(",")), {}
+    else:
+        stack_tuning, stack_cands = autotune.tune_stack(
+            lambda t: ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=t, xs=xs, device=dev))
     S = ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=stack_tuning, xs=xs, device=dev)
     # correctness gate before timing: bit-exact against the host int64 matvec
     S.run()
@@ -439,6 +442,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="", help="fixed stack launch parameters warps,ilp,depth,ctas_per_sm "
+                                                  "(default: autotuned)")
     ap.add_argument("--profile", action="store_true",
                     help="run the correctness gate and two steps only (the case ncu captures)")
     args = ap.parse_args()

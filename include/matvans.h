@@ -179,9 +179,9 @@ typedef struct mv_q8_tuning {
     int32_t warps, ilp, depth, ctas_per_sm;
 } mv_q8_tuning;
 
-/* mv_q8_matvec with explicit launch parameters (needs cols % 4 == 0 and a
- * 4-byte aligned x; mv_q8_matvec itself falls back to a non-persistent kernel
- * otherwise). */
+/* mv_q8_matvec with explicit launch parameters (needs cols % 16 == 0,
+ * seg_quads % 4 == 0 and a 16-byte aligned x; mv_q8_matvec itself falls back
+ * to a non-persistent kernel otherwise). */
 mv_status mv_q8_matvec_tuned(const mv_q8_view *m, const int8_t *x_dev, int batch, int32_t *y_dev,
                              const float *row_scales_dev, float *y_scaled_dev,
                              const mv_q8_tuning *tuning, void *stream);

@@ -155,14 +155,14 @@ static mv_status q8_encode(const int8_t *W, int rows, int cols, int local, int s
     e.stripes = (rows + 31) / 32;
     e.local = local != 0;
     if (seg_quads <= 0) {
-        // enough (stripe, segment) units to fill 148 SMs x 16 warps, segments
-        // of 64..128 quads when the row is long enough
+        // segments of 32..64 quads (a multiple of 4), as many as it takes to give
+        // 148 SMs x 16 warps at least one (stripe, segment) each
         int64_t want = (2368 + e.stripes - 1) / e.stripes;
-        int64_t lo = (e.qtot + 127) / 128, hi = std::max(1, e.qtot / 64);
+        int64_t lo = (e.qtot + 63) / 64, hi = std::max(1, e.qtot / 32);
         int64_t nseg = std::max(lo, std::min(want, hi));
-        if (nseg > 8) nseg = std::min<int64_t>((nseg + 7) / 8 * 8, std::max<int64_t>(hi, lo));
         nseg = std::max<int64_t>(1, std::min<int64_t>(nseg, e.qtot));
         seg_quads = (int)((e.qtot + nseg - 1) / nseg);
+        if (seg_quads < e.qtot) seg_quads = (seg_quads + 3) & ~3;
     }
     e.seg_quads = std::min(seg_quads, e.qtot);
     e.nseg = (e.qtot + e.seg_quads - 1) / e.seg_quads;

@@ -117,6 +117,22 @@ __device__ __forceinline__ void load_x(const int8_t *x, int cols, int q, uint32_
         xv[v] = __ldg(reinterpret_cast<const uint32_t *>(x + (size_t)v * cols) + q);
 }
 
+// Four consecutive quads of x (16 bytes) per vector; q % 4 == 0.
+template <int NV>
+__device__ __forceinline__ void load_x4(const int8_t *x, int cols, int q, uint4 (&xv)[NV]) {
+#pragma unroll
+    for (int v = 0; v < NV; v++) xv[v] = __ldg(reinterpret_cast<const uint4 *>(x + (size_t)v * cols + 4 * q));
+}
+
+template <int NV>
+__device__ __forceinline__ void dot4(uint32_t w, const uint4 (&xv)[NV], int j, int (&acc)[NV]) {
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+        const uint32_t xw = j == 0 ? xv[v].x : j == 1 ? xv[v].y : j == 2 ? xv[v].z : xv[v].w;
+        acc[v] = __dp4a((int)w, (int)xw, acc[v]);
+    }
+}
+
 // One decode step of one stream; returns the packed four symbols.
 __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t &kidx, const uint32_t kend,
                                             const uint32_t *buf, const uint32_t *lut_l, uint32_t stride,
@@ -250,6 +266,8 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
                 uint32_t loA = sb[lane], hiA = sb[32 + lane], kA = 64 + lane, PA = 0;
                 const uint32_t kendA = rows_now[0] * 32 + lane;
                 const int8_t *x = J.x;
+                const int cols = m.cols;
+                int iA = 0;
                 if (ILP == 2) {
                     uint32_t *sbB = sb + L.buf_words;
                     const int segB = segA + W;
@@ -257,45 +275,43 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
                     const int nqB = rows_now[ILP - 1] ? min(m.seg_quads, qtot - q0B) : 0;
                     uint32_t loB = sbB[lane], hiB = sbB[32 + lane], kB = 64 + lane, PB = 0;
                     const uint32_t kendB = rows_now[ILP - 1] * 32 + lane;
-                    const int nboth = min(nqA, nqB);
-                    int i = 0;
-#pragma unroll 2
-                    for (; i < nboth; i++) {
-                        uint32_t xa[NV], xb[NV];
-                        load_x<NV>(x, m.cols, q0A + i, xa);
-                        load_x<NV>(x, m.cols, q0B + i, xb);
-                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-                        const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+                    const int nboth = min(nqA, nqB) & ~3;
+                    for (; iA < nboth; iA += 4) {
+                        uint4 xa[NV], xb[NV];
+                        load_x4<NV>(x, cols, q0A + iA, xa);
+                        load_x4<NV>(x, cols, q0B + iA, xb);
 #pragma unroll
-                        for (int v = 0; v < NV; v++) {
-                            acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
-                            acc[v] = __dp4a((int)wb, (int)xb[v], acc[v]);
+                        for (int j = 0; j < 4; j++) {
+                            const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+                            const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+                            dot4<NV>(wa, xa, j, acc);
+                            dot4<NV>(wb, xb, j, acc);
                         }
                     }
-                    for (int j = i; j < nqA; j++) {
-                        uint32_t xa[NV];
-                        load_x<NV>(x, m.cols, q0A + j, xa);
-                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-#pragma unroll
-                        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
-                    }
-                    for (int j = i; j < nqB; j++) {
+                    for (int j = iA; j < nqB; j++) {
                         uint32_t xb[NV];
-                        load_x<NV>(x, m.cols, q0B + j, xb);
+                        load_x<NV>(x, cols, q0B + j, xb);
                         const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
 #pragma unroll
                         for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wb, (int)xb[v], acc[v]);
                     }
                     if (nqB > 0 && (hiB != 0 || loB != PB)) atomicOr(L.status, MV_DEV_FINAL_STATE);
-                } else {
-#pragma unroll 4
-                    for (int i = 0; i < nqA; i++) {
-                        uint32_t xa[NV];
-                        load_x<NV>(x, m.cols, q0A + i, xa);
-                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+                }
+                for (; iA + 4 <= nqA; iA += 4) {
+                    uint4 xa[NV];
+                    load_x4<NV>(x, cols, q0A + iA, xa);
 #pragma unroll
-                        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
+                    for (int j = 0; j < 4; j++) {
+                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+                        dot4<NV>(wa, xa, j, acc);
                     }
+                }
+                for (; iA < nqA; iA++) {
+                    uint32_t xa[NV];
+                    load_x<NV>(x, cols, q0A + iA, xa);
+                    const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+#pragma unroll
+                    for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
                 }
                 if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
             }
@@ -428,7 +444,7 @@ void plan_job(Q8Job &J, const mv_q8_tuning &t, uint32_t &item) {
 }  // namespace
 
 bool q8s_supports(const mv_q8_view *m, const int8_t *x) {
-    return (m->cols & 3) == 0 && ((uintptr_t)x & 3) == 0;
+    return (m->cols & 15) == 0 && ((uintptr_t)x & 15) == 0 && (m->seg_quads & 3) == 0;
 }
 
 // Single matrix through the persistent kernel (one inline job).
@@ -485,8 +501,12 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
     info->tbl_stripe_max = 2;
     for (int j = 0; j < njobs; j++) {
         const mv_q8_view &m = jobs[j].m;
-        if (m.rows <= 0 || m.cols <= 0 || (m.cols & 3) || m.nseg <= 0 || m.seg_quads <= 0)
-            return mv::fail(MV_ERR_ARG, "mv_q8_stack_plan: job %d has a bad view (cols %% 4 must be 0)", j);
+        if (m.rows <= 0 || m.cols <= 0 || (m.cols & 15) || m.nseg <= 0 || m.seg_quads <= 0 || (m.seg_quads & 3) ||
+            ((uintptr_t)jobs[j].x & 15))
+            return mv::fail(MV_ERR_ARG,
+                            "mv_q8_stack_plan: job %d: needs cols %% 16 == 0, seg_quads %% 4 == 0 and a "
+                            "16-byte aligned x",
+                            j);
         if ((uint64_t)item + (uint64_t)((m.rows + 31) / 32) * (uint64_t)m.nseg > 0xFFFFFFFFull)
             return mv::fail(MV_ERR_SHAPE, "mv_q8_stack_plan: too many work items");
         mv::plan_job(jobs[j], t, item);
@@ -537,7 +557,8 @@ mv_status mv_q8_matvec_tuned(const mv_q8_view *m, const int8_t *x_dev, int batch
     if (!m || !x_dev || !y_dev || batch <= 0) return mv::fail(MV_ERR_ARG, "mv_q8_matvec_tuned: bad arguments");
     if (y_scaled_dev && !row_scales_dev) return mv::fail(MV_ERR_ARG, "mv_q8_matvec_tuned: y_scaled needs scales");
     if (!mv::q8s_supports(m, x_dev))
-        return mv::fail(MV_ERR_ARG, "mv_q8_matvec_tuned: needs cols %% 4 == 0 and 4-byte aligned x");
+        return mv::fail(MV_ERR_ARG,
+                        "mv_q8_matvec_tuned: needs cols %% 16 == 0, seg_quads %% 4 == 0 and 16-byte aligned x");
     return mv::q8s_matvec(m, x_dev, batch, y_dev, row_scales_dev, y_scaled_dev, tuning, (cudaStream_t)stream);
 }
 

@@ -48,13 +48,17 @@ def test_q8_round_trip(name):
 
 
 def test_q8_bits_per_weight_near_entropy():
+    # with 128-quad segments the per-segment 64-bit state costs 0.125 bit/weight;
+    # the automatic choice shortens segments on small matrices to fill the GPU
     rng = np.random.default_rng(5)
     W = gauss(rng, 4, (256, 4096))
     H = codec.entropy_bits(W)
-    g = codec.q8_encode(W, local=False)
-    l = codec.q8_encode(W, local=True)
-    assert H < g["bits_per_weight"] < H + 0.45
-    assert H < l["bits_per_weight"] < H + 0.7
+    g = codec.q8_encode(W, local=False, seg_quads=128)
+    l = codec.q8_encode(W, local=True, seg_quads=128)
+    assert H < g["bits_per_weight"] < H + 0.3
+    assert H < l["bits_per_weight"] < H + 0.5
+    auto = codec.q8_encode(W, local=False)
+    assert auto["seg_quads"] % 4 == 0 and auto["bits_per_weight"] < H + 0.6
 
 
 def test_q8_auto_segments():
@@ -62,4 +66,6 @@ def test_q8_auto_segments():
     e = codec.q8_encode(W[:, :64], local=False)
     assert e["nseg"] == 1
     e = codec.q8_encode(np.zeros((128, 4096), np.int8), local=False)
-    assert 64 <= e["seg_quads"] <= 128
+    assert 32 <= e["seg_quads"] <= 64 and e["seg_quads"] % 4 == 0
+    e = codec.q8_encode(np.zeros((11008, 4096), np.int8), local=False)
+    assert e["seg_quads"] == 64
