@@ -29,7 +29,7 @@ TUNINGS = [(w, ilp, d, 0) for w in (1, 4, 8) for ilp in (1, 2) for d in (1, 2)] 
 @pytest.mark.parametrize("tuning", TUNINGS)
 def test_q8_persistent_all_tunings(tuning):
     rng = np.random.default_rng(sum(tuning))
-    for shape, local in (((100, 1000), True), ((257, 2048), False), ((64, 4096), True)):
+    for shape, local in (((100, 1008), True), ((257, 2048), False), ((64, 4096), True)):
         W = gauss(rng, 3.0, shape)
         M = ops.Q8Matrix.encode(W, local=local)
         for B in (1, 3, 8, 16, 20):
@@ -42,9 +42,18 @@ def test_q8_persistent_all_tunings(tuning):
     assert ops.device_status() == 0
 
 
+def test_q8_tuned_rejects_unsupported_shapes():
+    W = np.zeros((64, 1000), np.int8)
+    M = ops.Q8Matrix.encode(W)
+    with pytest.raises(_lib.MatvansError):
+        M.matvec(torch.zeros((1, 1000), dtype=torch.int8), tuning=(8, 2, 1, 0))
+    # the default entry point falls back to the general kernel for the same matrix
+    assert M.matvec(torch.ones((1, 1000), dtype=torch.int8)).abs().sum().item() == 0
+
+
 def test_q8_stack_uneven_shapes_one_launch():
     rng = np.random.default_rng(42)
-    shapes = [(512, 512), (1376, 512), (512, 1376), (96, 4096), (4096, 96), (33, 200)]
+    shapes = [(512, 512), (1376, 512), (512, 1376), (96, 4096), (4096, 96), (33, 208)]
     Ws, Ms = [], []
     for i, sh in enumerate(shapes):
         if i % 3 == 2:  # Laplace with rare +-100 outliers
