@@ -174,9 +174,12 @@ mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int3
  *   ilp          independent segments decoded per warp (1 or 2, default 2)
  *   depth        shared-memory stream buffers per warp (1 or 2, default 1):
  *                2 keeps the next work item's bulk copies in flight
- *   ctas_per_sm  cap on resident CTAs per SM (default: occupancy limit) */
+ *   ctas_per_sm  cap on resident CTAs per SM (default: occupancy limit)
+ *   parts        work items per 32-row stripe (its segments split in `parts`
+ *                ranges; default: whole stripes in stacks, enough parts to
+ *                fill the GPU for a single matrix) */
 typedef struct mv_q8_tuning {
-    int32_t warps, ilp, depth, ctas_per_sm;
+    int32_t warps, ilp, depth, ctas_per_sm, parts;
 } mv_q8_tuning;
 
 /* mv_q8_matvec with explicit launch parameters (needs cols % 16 == 0,

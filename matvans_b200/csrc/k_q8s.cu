@@ -76,20 +76,56 @@ __device__ __forceinline__ ItemInfo find_item(const Q8SLaunch &L, uint32_t it) {
     return ItemInfo{lo, (int)(rel / ng), (int)(rel % ng)};
 }
 
-// Issue the bulk copies of one warp's segment(s) of an item (lane 0 only).
+// Segment range [sb, se) of an item: its stripe's segments split into ngroups parts.
+__device__ __forceinline__ void item_segs(const mv_q8_view &m, int ngroups, int group, int &sb, int &se) {
+    const int spp = (m.nseg + ngroups - 1) / ngroups;
+    sb = group * spp;
+    se = min(m.nseg, sb + spp);
+}
+
+// Steps of a warp in an item of n segments; step j covers segments
+// sb + warp + j*W*ILP + k*W for k < ILP.
+__device__ __forceinline__ int warp_steps(int n, int warp, int W, int ILP) {
+    return warp < n ? (n - warp + W * ILP - 1) / (W * ILP) : 0;
+}
+
+// The next (item, step) of one warp's stream of segments, tracked by lane 0.
+struct StepCursor {
+    uint32_t it;
+    int j, steps, sb, se, stripe, job;
+};
+
+__device__ __forceinline__ void cursor_seek(StepCursor &c, const Q8SLaunch &L, uint32_t it, int warp, int W,
+                                            int ILP) {
+    for (; it < L.nitems; it += gridDim.x) {
+        const ItemInfo I = find_item(L, it);
+        const Q8Job &J = job_at(L, I.job);
+        int sb, se;
+        item_segs(J.m, J.ngroups, I.group, sb, se);
+        const int steps = warp_steps(se - sb, warp, W, ILP);
+        if (steps > 0) {
+            c = StepCursor{it, 0, steps, sb, se, I.stripe, I.job};
+            return;
+        }
+    }
+    c.it = L.nitems;
+}
+
+// Issue the bulk copies of the cursor's step into one slot (lane 0 only).
 template <int ILP>
-__device__ __forceinline__ void issue_item_copies(const Q8SLaunch &L, const Q8Job &J, const ItemInfo &I, int warp,
-                                                  int W, uint32_t *slot_bufs, uint64_t *bar, uint32_t *blk_rows) {
-    const mv_q8_view &m = J.m;
+__device__ __forceinline__ void issue_step(const Q8SLaunch &L, const StepCursor &c, int warp, int W,
+                                           uint32_t *slot_bufs, uint64_t *bar, uint32_t *rows_out) {
+    const mv_q8_view &m = job_at(L, c.job).m;
+    const int seg0 = c.sb + warp + c.j * W * ILP;
     uint32_t total = 0;
     uint32_t o0s[ILP], rows[ILP];
 #pragma unroll
     for (int k = 0; k < ILP; k++) {
-        const int seg = I.group * W * ILP + k * W + warp;
+        const int seg = seg0 + k * W;
         rows[k] = 0;
         o0s[k] = 0;
-        if (seg < m.nseg) {
-            const int b = I.stripe * m.nseg + seg;
+        if (seg < c.se) {
+            const int b = c.stripe * m.nseg + seg;
             const uint32_t o0 = __ldg(m.blk_off + b), o1 = __ldg(m.blk_off + b + 1);
             const uint32_t r = o1 - o0;
             if (o1 < o0 || o1 > m.blocks_rows || r < 2 || (int)r + 1 > L.buf_words / 32) {
@@ -100,7 +136,7 @@ __device__ __forceinline__ void issue_item_copies(const Q8SLaunch &L, const Q8Jo
                 total += r * 128u;
             }
         }
-        blk_rows[k] = rows[k];
+        rows_out[k] = rows[k];
     }
     mbar_arrive_expect_tx(bar, total);
     if (!L.drop_copy) {
@@ -138,11 +174,10 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
                                             const uint32_t *buf, const uint32_t *lut_l, uint32_t stride,
                                             uint32_t &P) {
     const uint32_t w = buf[kidx];
-    if (hi == 0) {
-        hi = lo;
-        lo = w;
-        kidx = min(kidx + 32, kend);
-    }
+    const bool need = hi == 0;
+    hi = need ? lo : hi;
+    lo = need ? w : lo;
+    kidx = need ? min(kidx + 32, kend) : kidx;
     const uint32_t a0 = __byte_perm(lo, 0, 0x4440), a1 = __byte_perm(lo, 0, 0x4441);
     const uint32_t a2 = __byte_perm(lo, 0, 0x4442), a3 = __byte_perm(lo, 0, 0x4443);
     // stride is 32 words, passed at run time so the index math stays an IMAD
@@ -164,56 +199,113 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
     return __byte_perm(__byte_perm(e0, e1, 0x0051), __byte_perm(e2, e3, 0x0051), 0x5410);
 }
 
+// Decode the ILP segments of one step into acc.
+template <int NV, int ILP>
+__device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view &m, const int8_t *x, int seg0, int W,
+                                            const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
+                                            int lane, int (&acc)[NV]) {
+    const int qtot = (m.cols + 3) >> 2;
+    const int q0A = seg0 * m.seg_quads;
+    const int nqA = rows_now[0] ? min(m.seg_quads, qtot - q0A) : 0;
+    uint32_t loA = sb[lane], hiA = sb[32 + lane], kA = 64 + lane, PA = 0;
+    const uint32_t kendA = rows_now[0] * 32 + lane;
+    const int cols = m.cols;
+    int iA = 0;
+    if (ILP == 2) {
+        uint32_t *sbB = sb + L.buf_words;
+        const int q0B = (seg0 + W) * m.seg_quads;
+        const int nqB = rows_now[ILP - 1] ? min(m.seg_quads, qtot - q0B) : 0;
+        uint32_t loB = sbB[lane], hiB = sbB[32 + lane], kB = 64 + lane, PB = 0;
+        const uint32_t kendB = rows_now[ILP - 1] * 32 + lane;
+        const int nboth = min(nqA, nqB) & ~3;
+        for (; iA < nboth; iA += 4) {
+            uint4 xa[NV], xb[NV];
+            load_x4<NV>(x, cols, q0A + iA, xa);
+            load_x4<NV>(x, cols, q0B + iA, xb);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+                const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+                dot4<NV>(wa, xa, j, acc);
+                dot4<NV>(wb, xb, j, acc);
+            }
+        }
+        for (int j = iA; j < nqB; j++) {
+            uint32_t xb[NV];
+            load_x<NV>(x, cols, q0B + j, xb);
+            const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+#pragma unroll
+            for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wb, (int)xb[v], acc[v]);
+        }
+        if (nqB > 0 && (hiB != 0 || loB != PB)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+    }
+    for (; iA + 4 <= nqA; iA += 4) {
+        uint4 xa[NV];
+        load_x4<NV>(x, cols, q0A + iA, xa);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+            dot4<NV>(wa, xa, j, acc);
+        }
+    }
+    for (; iA < nqA; iA++) {
+        uint32_t xa[NV];
+        load_x<NV>(x, cols, q0A + iA, xa);
+        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
+    }
+    if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+}
+
 template <int NV, int ILP, int DEPTH>
 __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = blockDim.x >> 5;
 
-    uint32_t *lut = reinterpret_cast<uint32_t *>(smem);                      // 8192 words
-    uint32_t *bufs = lut + 256 * 32;                                          // [W][DEPTH][ILP][buf_words]
-    int *red = reinterpret_cast<int *>(bufs + (size_t)W * DEPTH * ILP * L.buf_words);  // [W][NV][32]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(red + W * NV * 32);         // [W][DEPTH]
-    uint32_t *toff_s = reinterpret_cast<uint32_t *>(bars + W * DEPTH);        // [36]
-    uint32_t *rows_s = toff_s + 36;                                           // [W][DEPTH][ILP]
-    uint16_t *tsm = reinterpret_cast<uint16_t *>(rows_s + W * DEPTH * ILP);  // [tbl_stage]
-    uint32_t *my_rows = rows_s + warp * DEPTH * ILP;
+    uint32_t *lut = reinterpret_cast<uint32_t *>(smem);                                 // 8192 words
+    uint32_t *bufs = lut + 256 * 32;                                                     // [W][DEPTH][ILP][buf]
+    int *red = reinterpret_cast<int *>(bufs + (size_t)W * DEPTH * ILP * L.buf_words);    // [W][NV][32]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(red + W * NV * 32);                    // [W][DEPTH]
+    uint32_t *toff_s = reinterpret_cast<uint32_t *>(bars + W * DEPTH);                   // [36]
+    uint32_t *rows_s = toff_s + 36;                                                      // [W][DEPTH][ILP]
+    uint16_t *tsm = reinterpret_cast<uint16_t *>(rows_s + W * DEPTH * ILP);             // [tbl_stage]
 
     uint32_t *my_bufs = bufs + (size_t)warp * DEPTH * ILP * L.buf_words;
+    uint32_t *my_rows = rows_s + warp * DEPTH * ILP;
+    uint64_t *my_bars = bars + warp * DEPTH;
     if (lane == 0)
-        for (int d = 0; d < DEPTH; d++) mbar_init(&bars[warp * DEPTH + d], 1);
+        for (int d = 0; d < DEPTH; d++) mbar_init(&my_bars[d], 1);
     fence_mbar_init();
     __syncwarp();
 
-    const uint32_t G = gridDim.x;
-    // prologue: copies of the first item (and the second with DEPTH = 2)
-    for (int d = 0; d < DEPTH; d++) {
-        const uint32_t it = blockIdx.x + d * G;
-        if (lane == 0) {
-            for (int k = 0; k < ILP; k++) my_rows[d * ILP + k] = 0;
-            if (it < L.nitems) {
-                const ItemInfo I = find_item(L, it);
-                issue_item_copies<ILP>(L, job_at(L, I.job), I, warp, W, my_bufs + d * ILP * L.buf_words,
-                                       &bars[warp * DEPTH + d], my_rows + d * ILP);
-            }
+    // this warp's stream of (item, step) copies runs DEPTH steps ahead of its decode
+    StepCursor cur{};
+    uint32_t issued = 0;
+    if (lane == 0) {
+        cursor_seek(cur, L, blockIdx.x, warp, W, ILP);
+        for (int d = 0; d < DEPTH && cur.it < L.nitems; d++) {
+            const int slot = issued % DEPTH;
+            issue_step<ILP>(L, cur, warp, W, my_bufs + slot * ILP * L.buf_words, &my_bars[slot],
+                            my_rows + slot * ILP);
+            issued++;
+            if (++cur.j >= cur.steps) cursor_seek(cur, L, cur.it + gridDim.x, warp, W, ILP);
         }
     }
     __syncwarp();
 
     int lut_job = -1, lut_stripe = -1;
-    uint32_t iter = 0;
+    uint32_t consumed = 0;
     const uint32_t *lut_l = lut + lane;
-    for (uint32_t it = blockIdx.x; it < L.nitems; it += G, iter++) {
-        const int slot = DEPTH == 2 ? (int)(iter & 1) : 0;
-        const uint32_t parity = DEPTH == 2 ? ((iter >> 1) & 1) : (iter & 1);
+    for (uint32_t it = blockIdx.x; it < L.nitems; it += gridDim.x) {
         const ItemInfo I = find_item(L, it);
         const Q8Job &J = job_at(L, I.job);
         const mv_q8_view &m = J.m;
-        uint32_t rows_now[ILP];
-#pragma unroll
-        for (int k = 0; k < ILP; k++) rows_now[k] = my_rows[slot * ILP + k];
+        int sbeg, send;
+        item_segs(m, J.ngroups, I.group, sbeg, send);
 
-        // decode table (uniform decision across the CTA)
+        // decode table, rebuilt only when it changes (uniform across the CTA)
         if (I.job != lut_job || (m.local && I.stripe != lut_stripe)) {
             __syncthreads();  // every warp is done with the previous table
             const uint32_t r0 = m.local ? (uint32_t)I.stripe * 32 : 0;
@@ -251,83 +343,36 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
         int acc[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = 0;
-        const int qtot = (m.cols + 3) >> 2;
-        uint32_t *sb = my_bufs + slot * ILP * L.buf_words;
-        bool have_any = false;
+        const int steps = warp_steps(send - sbeg, warp, W, ILP);
+        for (int j = 0; j < steps; j++) {
+            const int slot = consumed % DEPTH;
+            const uint32_t parity = (consumed / DEPTH) & 1;
+            uint32_t rows_now[ILP];
+            bool any = false;
 #pragma unroll
-        for (int k = 0; k < ILP; k++) have_any |= rows_now[k] != 0;
-        if (have_any) {
-            if (!mbar_wait_bounded(&bars[warp * DEPTH + slot], parity, L.status, L.spin_limit)) {
-                mbar_wait_bounded(&bars[warp * DEPTH + slot], parity, nullptr, L.spin_limit);
-            } else {
-                const int segA = I.group * W * ILP + warp;
-                const int q0A = segA * m.seg_quads;
-                const int nqA = rows_now[0] ? min(m.seg_quads, qtot - q0A) : 0;
-                uint32_t loA = sb[lane], hiA = sb[32 + lane], kA = 64 + lane, PA = 0;
-                const uint32_t kendA = rows_now[0] * 32 + lane;
-                const int8_t *x = J.x;
-                const int cols = m.cols;
-                int iA = 0;
-                if (ILP == 2) {
-                    uint32_t *sbB = sb + L.buf_words;
-                    const int segB = segA + W;
-                    const int q0B = segB * m.seg_quads;
-                    const int nqB = rows_now[ILP - 1] ? min(m.seg_quads, qtot - q0B) : 0;
-                    uint32_t loB = sbB[lane], hiB = sbB[32 + lane], kB = 64 + lane, PB = 0;
-                    const uint32_t kendB = rows_now[ILP - 1] * 32 + lane;
-                    const int nboth = min(nqA, nqB) & ~3;
-                    for (; iA < nboth; iA += 4) {
-                        uint4 xa[NV], xb[NV];
-                        load_x4<NV>(x, cols, q0A + iA, xa);
-                        load_x4<NV>(x, cols, q0B + iA, xb);
-#pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-                            const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
-                            dot4<NV>(wa, xa, j, acc);
-                            dot4<NV>(wb, xb, j, acc);
-                        }
-                    }
-                    for (int j = iA; j < nqB; j++) {
-                        uint32_t xb[NV];
-                        load_x<NV>(x, cols, q0B + j, xb);
-                        const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
-#pragma unroll
-                        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wb, (int)xb[v], acc[v]);
-                    }
-                    if (nqB > 0 && (hiB != 0 || loB != PB)) atomicOr(L.status, MV_DEV_FINAL_STATE);
-                }
-                for (; iA + 4 <= nqA; iA += 4) {
-                    uint4 xa[NV];
-                    load_x4<NV>(x, cols, q0A + iA, xa);
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-                        dot4<NV>(wa, xa, j, acc);
-                    }
-                }
-                for (; iA < nqA; iA++) {
-                    uint32_t xa[NV];
-                    load_x<NV>(x, cols, q0A + iA, xa);
-                    const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-#pragma unroll
-                    for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
-                }
-                if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+            for (int k = 0; k < ILP; k++) {
+                rows_now[k] = my_rows[slot * ILP + k];
+                any |= rows_now[k] != 0;
             }
-        }
-        __syncwarp();
-        // this warp's slot is free again: start the copies of the item that will use it
-        if (lane == 0) {
-            const uint32_t nx = it + DEPTH * G;
-            for (int k = 0; k < ILP; k++) my_rows[slot * ILP + k] = 0;
-            if (nx < L.nitems) {
-                const ItemInfo N = find_item(L, nx);
-                issue_item_copies<ILP>(L, job_at(L, N.job), N, warp, W, sb, &bars[warp * DEPTH + slot],
-                                       my_rows + slot * ILP);
+            if (any) {
+                if (mbar_wait_bounded(&my_bars[slot], parity, L.status, L.spin_limit)) {
+                    decode_step<NV, ILP>(L, m, J.x, sbeg + warp + j * W * ILP, W, rows_now,
+                                         my_bufs + slot * ILP * L.buf_words, lut_l, lane, acc);
+                } else {
+                    mbar_wait_bounded(&my_bars[slot], parity, nullptr, L.spin_limit);
+                }
             }
+            __syncwarp();
+            consumed++;
+            // the slot is free: refill it with the step DEPTH ahead in this warp's stream
+            if (lane == 0 && cur.it < L.nitems) {
+                const int s2 = issued % DEPTH;
+                issue_step<ILP>(L, cur, warp, W, my_bufs + s2 * ILP * L.buf_words, &my_bars[s2], my_rows + s2 * ILP);
+                issued++;
+                if (++cur.j >= cur.steps) cursor_seek(cur, L, cur.it + gridDim.x, warp, W, ILP);
+            }
+            __syncwarp();
         }
-        __syncwarp();
 
         // reduce the W partials of each row of the stripe
 #pragma unroll
@@ -423,8 +468,9 @@ mv_status launch_q8s(const Q8SLaunch &L, int nv, const mv_q8_tuning &t, cudaStre
 int nv_round(int nb) { return nb <= 2 ? nb : nb <= 4 ? 4 : nb <= 8 ? 8 : 16; }
 
 mv_q8_tuning resolve(const mv_q8_tuning *t) {
-    mv_q8_tuning r{8, 2, 1, 0};
+    mv_q8_tuning r{8, 2, 1, 0, 0};
     if (t) {
+        if (t->parts > 0) r.parts = t->parts;
         if (t->warps > 0) r.warps = std::min(8, t->warps);
         if (t->ilp == 1 || t->ilp == 2) r.ilp = t->ilp;
         if (t->depth == 1 || t->depth == 2) r.depth = t->depth;
@@ -433,9 +479,9 @@ mv_q8_tuning resolve(const mv_q8_tuning *t) {
     return r;
 }
 
-void plan_job(Q8Job &J, const mv_q8_tuning &t, uint32_t &item) {
-    const int sg = t.warps * t.ilp;
-    J.ngroups = (J.m.nseg + sg - 1) / sg;
+// parts = 0: whole stripes (stacks); otherwise split each stripe's segments into `parts`
+void plan_job(Q8Job &J, const mv_q8_tuning &t, uint32_t &item, int parts) {
+    J.ngroups = std::max(1, std::min(parts > 0 ? parts : 1, J.m.nseg));
     J.atomic = J.ngroups > 1;
     J.item0 = item;
     item += (uint32_t)((J.m.rows + 31) / 32) * (uint32_t)J.ngroups;
@@ -463,7 +509,11 @@ mv_status q8s_matvec(const mv_q8_view *m, const int8_t *x, int batch, int32_t *y
         L.job0.scales = scales;
         L.job0.ys = ys ? ys + (size_t)v0 * m->rows : nullptr;
         uint32_t items = 0;
-        plan_job(L.job0, t, items);
+        // a single matrix: split stripes so that every warp slot of the GPU gets work
+        const int stripes = (m->rows + 31) / 32;
+        const int sg = t.warps * t.ilp;
+        int parts = t.parts > 0 ? t.parts : std::max(1, std::min(m->nseg / sg, (3 * sm_count() + stripes - 1) / stripes));
+        plan_job(L.job0, t, items, parts);
         if (L.job0.atomic) L.job0.ys = nullptr;
         L.jobs = nullptr;
         L.njobs = 1;
@@ -509,7 +559,7 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
                             j);
         if ((uint64_t)item + (uint64_t)((m.rows + 31) / 32) * (uint64_t)m.nseg > 0xFFFFFFFFull)
             return mv::fail(MV_ERR_SHAPE, "mv_q8_stack_plan: too many work items");
-        mv::plan_job(jobs[j], t, item);
+        mv::plan_job(jobs[j], t, item, t.parts);
         info->max_blk_rows = std::max(info->max_blk_rows, m.max_blk_rows);
         info->tbl_stripe_max = std::max(info->tbl_stripe_max, m.tbl_stripe_max);
     }

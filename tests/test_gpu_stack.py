@@ -23,7 +23,8 @@ def clean_status():
     yield
 
 
-TUNINGS = [(w, ilp, d, 0) for w in (1, 4, 8) for ilp in (1, 2) for d in (1, 2)] + [(8, 2, 1, 1), (3, 2, 2, 2)]
+TUNINGS = [(w, ilp, d, 0) for w in (1, 4, 8) for ilp in (1, 2) for d in (1, 2)] + \
+    [(8, 2, 1, 1), (3, 2, 2, 2), (8, 1, 2, 0, 3), (4, 2, 2, 0, 1), (2, 1, 1, 0, 5)]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS)
@@ -65,7 +66,7 @@ def test_q8_stack_uneven_shapes_one_launch():
         Ws.append(W)
         Ms.append(ops.Q8Matrix.encode(W, local=(i % 2 == 0)))
     for B in (1, 4, 8, 16):
-        for tuning in ((0, 0, 0, 0), (4, 1, 2, 0)):
+        for tuning in ((0, 0, 0, 0), (4, 1, 2, 0), (8, 2, 2, 0, 2)):
             xs = [torch.from_numpy(rng.integers(-127, 128, size=(B, M.cols)).astype(np.int8)).cuda() for M in Ms]
             sc = [torch.from_numpy(rng.uniform(1e-3, 1e-2, size=M.rows).astype(np.float32)).cuda() for M in Ms]
             S = ops.Q8Stack(Ms, batch=B, tuning=tuning, xs=xs, scales=sc)
