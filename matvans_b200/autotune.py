@@ -22,7 +22,10 @@ import torch
 from . import _lib
 from ._lib import Q8Tuning
 
-CANDIDATES = [(w, ilp, d, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)]
+CANDIDATES = [(w, ilp, d, 0, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)]
+# single matrices additionally try splitting each stripe into more work items
+SINGLE_CANDIDATES = CANDIDATES + [(w, ilp, d, 0, p) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)
+                                  for p in (2, 4)]
 L2_BYTES = 126 * 2 ** 20
 _lock = threading.Lock()
 
@@ -94,7 +97,7 @@ def time_launches(fns, reps=10):
     return e0.elapsed_time(e1) / reps / len(fns)
 
 
-def tune(M, batch=1, candidates=CANDIDATES, reps=10, force=False):
+def tune(M, batch=1, candidates=SINGLE_CANDIDATES, reps=10, force=False):
     """Best Q8Tuning for matrix M at `batch` vectors (cached)."""
     k = key(M, batch)
     with _lock:

@@ -20,13 +20,14 @@
 //   * per-row partial sums are reduced across warps in shared memory and
 //     stored, or added with exact integer atomics when a row spans groups.
 //
-// Decode step (per lane, per quad of 4 symbols; table entry e = f | sym << 8
-// | r << 16 with f the symbol's frequency, r = q - cum):
+// Decode step (per lane, per quad of 4 symbols; table entry e = f | sym << 16
+// | r << 24 with f the symbol's frequency, r = q - cum < f <= 255):
 //   refill:   if (hi == 0) { hi = lo; lo = next word }
 //   lookups:  e_i = table[byte i of lo]
-//   update:   t2 = r2 + f2*r3, t1 = r1 + f1*t2 (dp2a: 16-bit x 8-bit dot
-//             products read f straight from the entry), t0 = r0 + f0*t1,
-//             P = (f0 f1)(f2 f3), (hi:lo) = hi*P + t0 (one 32x32->64 IMAD)
+//   update:   t2 = r2 + f2*r3, t1 = r1 + f1*t2, f0*f1, f2*f3 (dp2a: 16-bit x
+//             8-bit dot products read f straight from the entries), t0 =
+//             r0 + f0*t1, P = (f0 f1)(f2 f3), (hi:lo) = hi*P + t0 (one
+//             32x32->64 IMAD)
 #include <algorithm>
 #include <cstdio>
 
@@ -183,20 +184,19 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
     // stride is 32 words, passed at run time so the index math stays an IMAD
     const uint32_t e0 = lut_l[a0 * stride], e1 = lut_l[a1 * stride];
     const uint32_t e2 = lut_l[a2 * stride], e3 = lut_l[a3 * stride];
-    const uint32_t r0 = __umulhi(e0, 65536u), r1 = __umulhi(e1, 65536u);
-    const uint32_t r2 = e2 >> 16, r3 = e3 >> 16;
+    // entry = f | sym << 16 | r << 24 (byte 1 zero, so the low half-word is exactly f)
+    const uint32_t r0 = __umulhi(e0, 256u), r1 = __umulhi(e1, 256u);
+    const uint32_t r2 = e2 >> 24, r3 = e3 >> 24;
     const uint32_t t2 = __dp2a_lo(r3, e2, r2);      // r2 + f2*r3
     const uint32_t t1 = __dp2a_lo(t2, e1, r1);      // r1 + f1*t2  (t2 < 2^16)
-    const uint32_t f1 = e1 & 0xFF, f3 = e3 & 0xFF;
-    const uint32_t p01 = __dp2a_lo(f1, e0, 0u);     // f0*f1
-    const uint32_t p23 = __dp2a_lo(f3, e2, 0u);     // f2*f3
-    const uint32_t f0 = e0 & 0xFF;
+    const uint32_t p01 = __dp2a_lo(e1, e0, 0u);     // f1*f0 + (sym1 | r1 << 8) * 0
+    const uint32_t p23 = __dp2a_lo(e3, e2, 0u);     // f3*f2
     P = p01 * p23;
-    const uint32_t t0 = r0 + f0 * t1;
+    const uint32_t t0 = r0 + (e0 & 0xFFu) * t1;
     const unsigned long long s = (unsigned long long)hi * P + t0;
     lo = (uint32_t)s;
     hi = (uint32_t)(s >> 32);
-    return __byte_perm(__byte_perm(e0, e1, 0x0051), __byte_perm(e2, e3, 0x0051), 0x5410);
+    return __byte_perm(__byte_perm(e0, e1, 0x0062), __byte_perm(e2, e3, 0x0062), 0x5410);
 }
 
 // Decode the ILP segments of one step into acc.
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
                 const uint32_t ent = tsm[k];
                 const uint32_t f = ent >> 8, sym = ent & 0xFF;
                 const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
-                for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 8) | ((q - cum) << 16);
+                for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
                 cum += f;
             }
             if (cum < (uint32_t)qhi) {
