@@ -322,7 +322,8 @@ def run_ours(args):
         t_ms = info["us"] * 1e-3
         per[e["name"]] = {"us": 1e3 * t_ms, "int8_equiv_gbs": int8_equiv_bytes(e["rows"], e["cols"]) / t_ms / 1e6,
                           "compressed_gbs": e["alg_bytes"] / t_ms / 1e6, "bits_per_weight": M.bits_per_weight,
-                          "entropy_bits": e["entropy"], "tuning": [tun.warps, tun.ilp, tun.depth, tun.ctas_per_sm]}
+                          "entropy_bits": e["entropy"],
+                          "tuning": [tun.warps, tun.ilp, tun.depth, tun.ctas_per_sm, tun.parts]}
     torch.cuda.empty_cache()
     dense, cublas, awr_t, wpr_t = {}, {}, {}, {}
     for m in mats:
