@@ -226,6 +226,24 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
 mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info,
                              int batch, const mv_q8_tuning *tuning, void *stream);
 
+/* Float form (no reference counterpart): y[b][r] = s[r] * sum_c W[r][c] *
+ * x[b][c] with x bf16 [batch][cols] (16-byte aligned), fp32 accumulation in a
+ * fixed order (deterministic), fp32 y [batch][rows].  cols % 16 == 0.  Passes
+ * of up to 8 vectors share one decode. */
+mv_status mv_q8_matvec_bf16(const mv_q8_view *m, const uint16_t *x_dev, int batch,
+                            const float *row_scales_dev, float *y_dev, const mv_q8_tuning *tuning,
+                            void *stream);
+
+/* Transposed float form, the backward of the above: dx[b][c] = sum_r W[r][c]
+ * * s[r] * dy[b][r] with dy bf16 [batch][rows], fp32 dx [batch][cols]
+ * (zeroed by the call).  The streams are decoded again (W is never stored);
+ * the 32 rows of a stripe are summed per column inside the warp and stripes
+ * are combined with fp32 atomics, so the result is reproducible to fp32
+ * rounding, not bit for bit. */
+mv_status mv_q8_matvec_t_bf16(const mv_q8_view *m, const uint16_t *dy_dev, int batch,
+                              const float *row_scales_dev, float *dx_dev,
+                              const mv_q8_tuning *tuning, void *stream);
+
 /* Decode the whole matrix to W_dev[rows][cols] (test / debugging aid). */
 mv_status mv_q8_decode(const mv_q8_view *m, int8_t *W_dev, void *stream);
 

@@ -199,17 +199,207 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
     return __byte_perm(__byte_perm(e0, e1, 0x0062), __byte_perm(e2, e3, 0x0062), 0x5410);
 }
 
-// Decode the ILP segments of one step into acc.
-template <int NV, int ILP>
-__device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view &m, const int8_t *x, int seg0, int W,
+// --------------------------------------------------------------- consumers
+// A consumer turns decoded quads (four int8 weights of the lane's row) into
+// the kernel's output.  Per item it is set up (begin_item), fed groups of four
+// quads (load_group / use) and single tail quads (single), and closes the item
+// (finish_item, which may synchronise the CTA).
+
+// y = W x, int8 x, exact int32 y (+ optional fp32 s*y).
+template <int NV>
+struct IntCons {
+    static constexpr int kNV = NV;
+    const int8_t *x;
+    int cols;
+    int acc[NV];
+    struct Group {
+        uint4 xv[NV];
+    };
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &, const Q8Job &J, int, int) {
+        x = J.x;
+        cols = J.m.cols;
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = 0;
+    }
+    __device__ __forceinline__ void load_group(Group &g, int q) const { load_x4<NV>(x, cols, q, g.xv); }
+    __device__ __forceinline__ void use(const Group &g, int j, int, uint32_t wq, int) { dot4<NV>(wq, g.xv, j, acc); }
+    __device__ __forceinline__ void single(int q, uint32_t wq, int) {
+        uint32_t xv[NV];
+        load_x<NV>(x, cols, q, xv);
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wq, (int)xv[v], acc[v]);
+    }
+    __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
+                                                int W, void *red_smem) {
+        int *red = reinterpret_cast<int *>(red_smem);
+#pragma unroll
+        for (int v = 0; v < NV; v++) red[(warp * NV + v) * 32 + lane] = acc[v];
+        __syncthreads();
+        const mv_q8_view &m = J.m;
+        for (int t = threadIdx.x; t < NV * 32; t += blockDim.x) {
+            const int v = t >> 5, l = t & 31;
+            int sum = 0;
+            for (int w = 0; w < W; w++) sum += red[(w * NV + v) * 32 + l];
+            const int row = stripe * 32 + l;
+            if (row < m.rows && v < L.batch) {
+                int32_t *dst = J.y + (size_t)v * m.rows + row;
+                if (J.atomic) {
+                    atomicAdd(dst, sum);
+                } else {
+                    *dst = sum;
+                    if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
+                }
+            }
+        }
+        __syncthreads();  // red is reused by the next item
+    }
+};
+
+// four int8 weights (packed) -> fp32: the bytes biased by 128 are the low
+// mantissa bits of 2^23, so each conversion is one byte permute and one add
+__device__ __forceinline__ void i8x4_to_f32(uint32_t wq, float (&f)[4]) {
+    const uint32_t u = wq ^ 0x80808080u;
+    f[0] = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7650)) - 8388736.0f;
+    f[1] = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7651)) - 8388736.0f;
+    f[2] = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7652)) - 8388736.0f;
+    f[3] = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7653)) - 8388736.0f;
+}
+
+__device__ __forceinline__ float bf16_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t u) { return __uint_as_float(u & 0xFFFF0000u); }
+
+// Y = diag(s) W X with X bf16 [NV][cols], fp32 accumulation, fp32 Y [NV][rows] (J.ys).
+template <int NV>
+struct FwdCons {
+    static constexpr int kNV = NV;
+    const uint16_t *x;
+    int cols;
+    float acc[NV];
+    struct Group {
+        uint4 xv[NV][2];  // 16 bf16 = 4 quads
+    };
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &, const Q8Job &J, int, int) {
+        x = reinterpret_cast<const uint16_t *>(J.x);
+        cols = J.m.cols;
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = 0.f;
+    }
+    __device__ __forceinline__ void load_group(Group &g, int q) const {
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const uint4 *p = reinterpret_cast<const uint4 *>(x + (size_t)v * cols + 4 * q);
+            g.xv[v][0] = __ldg(p);
+            g.xv[v][1] = __ldg(p + 1);
+        }
+    }
+    __device__ __forceinline__ void fma4(uint32_t wq, uint32_t xa, uint32_t xb, float &a) {
+        float w[4];
+        i8x4_to_f32(wq, w);
+        a = fmaf(w[0], bf16_lo(xa), a);
+        a = fmaf(w[1], bf16_hi(xa), a);
+        a = fmaf(w[2], bf16_lo(xb), a);
+        a = fmaf(w[3], bf16_hi(xb), a);
+    }
+    __device__ __forceinline__ void use(const Group &g, int j, int, uint32_t wq, int) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const uint4 &h = g.xv[v][j >> 1];
+            const uint32_t xa = (j & 1) ? h.z : h.x, xb = (j & 1) ? h.w : h.y;
+            fma4(wq, xa, xb, acc[v]);
+        }
+    }
+    __device__ __forceinline__ void single(int q, uint32_t wq, int) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const uint2 xv = __ldg(reinterpret_cast<const uint2 *>(x + (size_t)v * cols + 4 * q));
+            fma4(wq, xv.x, xv.y, acc[v]);
+        }
+    }
+    __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
+                                                int W, void *red_smem) {
+        float *red = reinterpret_cast<float *>(red_smem);
+#pragma unroll
+        for (int v = 0; v < NV; v++) red[(warp * NV + v) * 32 + lane] = acc[v];
+        __syncthreads();
+        const mv_q8_view &m = J.m;
+        for (int t = threadIdx.x; t < NV * 32; t += blockDim.x) {
+            const int v = t >> 5, l = t & 31;
+            float sum = 0.f;
+            for (int w = 0; w < W; w++) sum += red[(w * NV + v) * 32 + l];  // fixed order: deterministic
+            const int row = stripe * 32 + l;
+            if (row < m.rows && v < L.batch) {
+                float *dst = J.ys + (size_t)v * m.rows + row;
+                const float val = sum * J.scales[row];
+                if (J.atomic) atomicAdd(dst, val);
+                else *dst = val;
+            }
+        }
+        __syncthreads();
+    }
+};
+
+// dX = W^T (s . dY): dY bf16 [NV][rows] (J.x), dX fp32 [NV][cols] (J.ys, zeroed,
+// accumulated with fp32 atomics across stripes).  The 32 lanes of a warp are
+// the 32 rows of the stripe, so the four column contributions of a quad are
+// summed over the lanes with a 5-step transpose-reduce (four values in, one
+// column sum in each group of 8 lanes out).
+template <int NV>
+struct BwdCons {
+    static constexpr int kNV = NV;
+    float g[NV];
+    float *dx;
+    int cols;
+    struct Group {};
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int lane) {
+        const int row = stripe * 32 + lane;
+        const uint16_t *dy = reinterpret_cast<const uint16_t *>(J.x);
+        dx = J.ys;
+        cols = J.m.cols;
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            float gv = 0.f;
+            if (row < J.m.rows && v < L.batch)
+                gv = J.scales[row] * __uint_as_float((uint32_t)__ldg(dy + (size_t)v * J.m.rows + row) << 16);
+            g[v] = gv;
+        }
+    }
+    __device__ __forceinline__ void load_group(Group &, int) const {}
+    __device__ __forceinline__ void scatter(int q, uint32_t wq, int lane) {
+        float w[4];
+        i8x4_to_f32(wq, w);
+        const bool b4 = lane & 16, b3 = lane & 8;
+        const int col = 4 * q + (b4 ? 2 : 0) + (b3 ? 1 : 0);
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const float a0 = w[0] * g[v], a1 = w[1] * g[v], a2 = w[2] * g[v], a3 = w[3] * g[v];
+            float k0 = b4 ? a2 : a0, k1 = b4 ? a3 : a1;
+            const float s0 = b4 ? a0 : a2, s1 = b4 ? a1 : a3;
+            k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+            k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+            float k = b3 ? k1 : k0;
+            const float sx = b3 ? k0 : k1;
+            k += __shfl_xor_sync(0xffffffffu, sx, 8);
+            k += __shfl_xor_sync(0xffffffffu, k, 4);
+            k += __shfl_xor_sync(0xffffffffu, k, 2);
+            k += __shfl_xor_sync(0xffffffffu, k, 1);
+            if ((lane & 7) == 0 && col < cols) atomicAdd(dx + (size_t)v * cols + col, k);
+        }
+    }
+    __device__ __forceinline__ void use(const Group &, int, int q, uint32_t wq, int lane) { scatter(q, wq, lane); }
+    __device__ __forceinline__ void single(int q, uint32_t wq, int lane) { scatter(q, wq, lane); }
+    __device__ __forceinline__ void finish_item(const Q8SLaunch &, const Q8Job &, int, int, int, int, void *) {}
+};
+
+// Decode the ILP segments of one step, feeding every quad to the consumer.
+template <class Cons, int ILP>
+__device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                            int lane, int (&acc)[NV]) {
+                                            int lane, Cons &cons) {
     const int qtot = (m.cols + 3) >> 2;
     const int q0A = seg0 * m.seg_quads;
     const int nqA = rows_now[0] ? min(m.seg_quads, qtot - q0A) : 0;
     uint32_t loA = sb[lane], hiA = sb[32 + lane], kA = 64 + lane, PA = 0;
     const uint32_t kendA = rows_now[0] * 32 + lane;
-    const int cols = m.cols;
     int iA = 0;
     if (ILP == 2) {
         uint32_t *sbB = sb + L.buf_words;
@@ -219,47 +409,42 @@ __device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view
         const uint32_t kendB = rows_now[ILP - 1] * 32 + lane;
         const int nboth = min(nqA, nqB) & ~3;
         for (; iA < nboth; iA += 4) {
-            uint4 xa[NV], xb[NV];
-            load_x4<NV>(x, cols, q0A + iA, xa);
-            load_x4<NV>(x, cols, q0B + iA, xb);
+            typename Cons::Group ga, gb;
+            cons.load_group(ga, q0A + iA);
+            cons.load_group(gb, q0B + iA);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
                 const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
-                dot4<NV>(wa, xa, j, acc);
-                dot4<NV>(wb, xb, j, acc);
+                cons.use(ga, j, q0A + iA + j, wa, lane);
+                cons.use(gb, j, q0B + iA + j, wb, lane);
             }
         }
         for (int j = iA; j < nqB; j++) {
-            uint32_t xb[NV];
-            load_x<NV>(x, cols, q0B + j, xb);
             const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
-#pragma unroll
-            for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wb, (int)xb[v], acc[v]);
+            cons.single(q0B + j, wb, lane);
         }
         if (nqB > 0 && (hiB != 0 || loB != PB)) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
     for (; iA + 4 <= nqA; iA += 4) {
-        uint4 xa[NV];
-        load_x4<NV>(x, cols, q0A + iA, xa);
+        typename Cons::Group ga;
+        cons.load_group(ga, q0A + iA);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-            dot4<NV>(wa, xa, j, acc);
+            cons.use(ga, j, q0A + iA + j, wa, lane);
         }
     }
     for (; iA < nqA; iA++) {
-        uint32_t xa[NV];
-        load_x<NV>(x, cols, q0A + iA, xa);
         const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-#pragma unroll
-        for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wa, (int)xa[v], acc[v]);
+        cons.single(q0A + iA, wa, lane);
     }
     if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
 }
 
-template <int NV, int ILP, int DEPTH>
+template <class Cons, int ILP, int DEPTH>
 __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
+    constexpr int NV = Cons::kNV;
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = blockDim.x >> 5;
@@ -340,9 +525,8 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
             lut_stripe = I.stripe;
         }
 
-        int acc[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) acc[v] = 0;
+        Cons cons;
+        cons.begin_item(L, J, I.stripe, lane);
         const int steps = warp_steps(send - sbeg, warp, W, ILP);
         for (int j = 0; j < steps; j++) {
             const int slot = consumed % DEPTH;
@@ -356,8 +540,8 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
             }
             if (any) {
                 if (mbar_wait_bounded(&my_bars[slot], parity, L.status, L.spin_limit)) {
-                    decode_step<NV, ILP>(L, m, J.x, sbeg + warp + j * W * ILP, W, rows_now,
-                                         my_bufs + slot * ILP * L.buf_words, lut_l, lane, acc);
+                    decode_step<Cons, ILP>(L, m, sbeg + warp + j * W * ILP, W, rows_now,
+                                           my_bufs + slot * ILP * L.buf_words, lut_l, lane, cons);
                 } else {
                     mbar_wait_bounded(&my_bars[slot], parity, nullptr, L.spin_limit);
                 }
@@ -374,26 +558,7 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
             __syncwarp();
         }
 
-        // reduce the W partials of each row of the stripe
-#pragma unroll
-        for (int v = 0; v < NV; v++) red[(warp * NV + v) * 32 + lane] = acc[v];
-        __syncthreads();
-        for (int t = threadIdx.x; t < NV * 32; t += blockDim.x) {
-            const int v = t >> 5, l = t & 31;
-            int sum = 0;
-            for (int w = 0; w < W; w++) sum += red[(w * NV + v) * 32 + l];
-            const int row = I.stripe * 32 + l;
-            if (row < m.rows && v < L.batch) {
-                int32_t *dst = J.y + (size_t)v * m.rows + row;
-                if (J.atomic) {
-                    atomicAdd(dst, sum);
-                } else {
-                    *dst = sum;
-                    if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
-                }
-            }
-        }
-        __syncthreads();  // red is reused by the next item
+        cons.finish_item(L, J, I.stripe, warp, lane, W, red);
     }
 }
 
@@ -428,13 +593,13 @@ size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage)
            36 * 4 + (size_t)W * DEPTH * ILP * 4 + (size_t)tbl_stage * 2;
 }
 
-template <int NV, int ILP, int DEPTH>
+template <class Cons, int ILP, int DEPTH>
 mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t st) {
-    const size_t smem = q8s_smem(NV, ILP, DEPTH, W, L.buf_words, L.tbl_stage);
+    const size_t smem = q8s_smem(Cons::kNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage);
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch needs %zu B of shared memory (max %d)", smem,
                     max_smem_optin());
-    auto kern = q8s_kernel<NV, ILP, DEPTH>;
+    auto kern = q8s_kernel<Cons, ILP, DEPTH>;
     int bps = 0;
     mv_status rc = prepare_kernel((const void *)kern, smem, 32 * W, &bps);
     if (rc) return rc;
@@ -445,23 +610,41 @@ mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t 
     return MV_OK;
 }
 
-template <int NV>
-mv_status launch_q8s_nv(const Q8SLaunch &L, const mv_q8_tuning &t, cudaStream_t st) {
+template <class Cons>
+mv_status launch_q8s_c(const Q8SLaunch &L, const mv_q8_tuning &t, cudaStream_t st) {
     if (t.ilp == 2) {
-        if (t.depth == 2) return launch_q8s_t<NV, 2, 2>(L, t.warps, t.ctas_per_sm, st);
-        return launch_q8s_t<NV, 2, 1>(L, t.warps, t.ctas_per_sm, st);
+        if (t.depth == 2) return launch_q8s_t<Cons, 2, 2>(L, t.warps, t.ctas_per_sm, st);
+        return launch_q8s_t<Cons, 2, 1>(L, t.warps, t.ctas_per_sm, st);
     }
-    if (t.depth == 2) return launch_q8s_t<NV, 1, 2>(L, t.warps, t.ctas_per_sm, st);
-    return launch_q8s_t<NV, 1, 1>(L, t.warps, t.ctas_per_sm, st);
+    if (t.depth == 2) return launch_q8s_t<Cons, 1, 2>(L, t.warps, t.ctas_per_sm, st);
+    return launch_q8s_t<Cons, 1, 1>(L, t.warps, t.ctas_per_sm, st);
 }
 
 mv_status launch_q8s(const Q8SLaunch &L, int nv, const mv_q8_tuning &t, cudaStream_t st) {
     switch (nv) {
-        case 1: return launch_q8s_nv<1>(L, t, st);
-        case 2: return launch_q8s_nv<2>(L, t, st);
-        case 4: return launch_q8s_nv<4>(L, t, st);
-        case 8: return launch_q8s_nv<8>(L, t, st);
-        default: return launch_q8s_nv<16>(L, t, st);
+        case 1: return launch_q8s_c<IntCons<1>>(L, t, st);
+        case 2: return launch_q8s_c<IntCons<2>>(L, t, st);
+        case 4: return launch_q8s_c<IntCons<4>>(L, t, st);
+        case 8: return launch_q8s_c<IntCons<8>>(L, t, st);
+        default: return launch_q8s_c<IntCons<16>>(L, t, st);
+    }
+}
+
+// mode 1: float forward, mode 2: float backward (transposed); nv in {1,2,4,8}
+mv_status launch_q8f(const Q8SLaunch &L, int mode, int nv, const mv_q8_tuning &t, cudaStream_t st) {
+    if (mode == 1) {
+        switch (nv) {
+            case 1: return launch_q8s_c<FwdCons<1>>(L, t, st);
+            case 2: return launch_q8s_c<FwdCons<2>>(L, t, st);
+            case 4: return launch_q8s_c<FwdCons<4>>(L, t, st);
+            default: return launch_q8s_c<FwdCons<8>>(L, t, st);
+        }
+    }
+    switch (nv) {
+        case 1: return launch_q8s_c<BwdCons<1>>(L, t, st);
+        case 2: return launch_q8s_c<BwdCons<2>>(L, t, st);
+        case 4: return launch_q8s_c<BwdCons<4>>(L, t, st);
+        default: return launch_q8s_c<BwdCons<8>>(L, t, st);
     }
 }
 
@@ -539,9 +722,72 @@ mv_status q8s_matvec(const mv_q8_view *m, const int8_t *x, int batch, int32_t *y
     return MV_OK;
 }
 
+// Float forward / transposed product through the persistent kernel.
+mv_status q8f_run(const mv_q8_view *m, int mode, const uint16_t *in, int batch, const float *scales, float *out,
+                  const mv_q8_tuning *tuning, cudaStream_t st) {
+    mv_status rc;
+    uint32_t *status = device_status_word(&rc);
+    if (rc) return rc;
+    const mv_q8_tuning t = resolve(tuning);
+    const int in_len = mode == 1 ? m->cols : m->rows;   // elements per vector in
+    const int out_len = mode == 1 ? m->rows : m->cols;  // elements per vector out
+    if (mode == 2) MV_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)batch * out_len, st), "memset(dx)");
+    for (int v0 = 0; v0 < batch; v0 += 8) {
+        const int nb = std::min(8, batch - v0);
+        Q8SLaunch L{};
+        L.job0.m = *m;
+        L.job0.x = reinterpret_cast<const int8_t *>(in + (size_t)v0 * in_len);
+        L.job0.y = nullptr;
+        L.job0.scales = scales;
+        L.job0.ys = out + (size_t)v0 * out_len;
+        uint32_t items = 0;
+        // forward: whole stripes (deterministic sums); backward: atomics anyway, so split for parallelism
+        int parts = 1;
+        if (mode == 2) {
+            const int stripes = (m->rows + 31) / 32, sg = t.warps * t.ilp;
+            parts = t.parts > 0 ? t.parts : std::max(1, std::min(m->nseg / sg, (3 * sm_count() + stripes - 1) / stripes));
+        }
+        plan_job(L.job0, t, items, parts);
+        if (mode == 1 && L.job0.atomic) return fail(MV_ERR_ARG, "float forward needs whole stripes (parts = 1)");
+        L.jobs = nullptr;
+        L.njobs = 1;
+        L.nitems = items;
+        L.batch = nb;
+        L.status = status;
+        L.spin_limit = wait_spin_limit();
+        L.drop_copy = inject_drop_copy();
+        L.buf_words = (m->max_blk_rows + 1) * 32;
+        L.tbl_stage = (int)((m->tbl_stripe_max + 7) & ~7u);
+        L.lut_stride = 32;
+        rc = launch_q8f(L, mode, nv_round(nb), t, st);
+        if (rc) return rc;
+    }
+    return MV_OK;
+}
+
 }  // namespace mv
 
 extern "C" {
+
+mv_status mv_q8_matvec_bf16(const mv_q8_view *m, const uint16_t *x_dev, int batch, const float *row_scales_dev,
+                            float *y_dev, const mv_q8_tuning *tuning, void *stream) {
+    if (!m || !x_dev || !row_scales_dev || !y_dev || batch <= 0)
+        return mv::fail(MV_ERR_ARG, "mv_q8_matvec_bf16: bad arguments");
+    if ((m->cols & 15) || ((uintptr_t)x_dev & 15) || (m->seg_quads & 3))
+        return mv::fail(MV_ERR_ARG, "mv_q8_matvec_bf16: needs cols %% 16 == 0, seg_quads %% 4 == 0, 16-byte aligned x");
+    mv_q8_tuning t = mv::resolve(tuning);
+    t.parts = 1;
+    return mv::q8f_run(m, 1, x_dev, batch, row_scales_dev, y_dev, &t, (cudaStream_t)stream);
+}
+
+mv_status mv_q8_matvec_t_bf16(const mv_q8_view *m, const uint16_t *dy_dev, int batch, const float *row_scales_dev,
+                              float *dx_dev, const mv_q8_tuning *tuning, void *stream) {
+    if (!m || !dy_dev || !row_scales_dev || !dx_dev || batch <= 0)
+        return mv::fail(MV_ERR_ARG, "mv_q8_matvec_t_bf16: bad arguments");
+    if ((m->cols & 15) || (m->seg_quads & 3))
+        return mv::fail(MV_ERR_ARG, "mv_q8_matvec_t_bf16: needs cols %% 16 == 0 and seg_quads %% 4 == 0");
+    return mv::q8f_run(m, 2, dy_dev, batch, row_scales_dev, dx_dev, tuning, (cudaStream_t)stream);
+}
 
 mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning, mv_q8_stack_info *info) {
     if (!jobs || njobs <= 0 || !info) return mv::fail(MV_ERR_ARG, "mv_q8_stack_plan: bad arguments");

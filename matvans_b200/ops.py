@@ -184,6 +184,38 @@ class Q8Matrix(_Matrix):
         check(lib().mv_q8_matvec_tuned(ctypes.byref(self._view), _p(x2), B, _p(y), _p(scales), _p(ys),
                                        ctypes.byref(t), _stream()))
 
+    def _tuning_ptr(self, tuning):
+        if tuning is None:
+            return None
+        t = tuning if isinstance(tuning, Q8Tuning) else Q8Tuning(*tuning)
+        self._last_tuning = t
+        return ctypes.byref(t)
+
+    def matvec_bf16(self, x, scales, out=None, tuning=None):
+        """Float form y = diag(scales) W x: x bf16 [B, cols] -> fp32 [B, rows]."""
+        x2 = x.reshape(1, -1) if x.dim() == 1 else x
+        if x2.dtype != torch.bfloat16 or x2.shape[-1] != self.cols:
+            raise ValueError(f"x must be bf16 with {self.cols} columns")
+        x2 = x2.to(self.device).contiguous()
+        s = scales.to(self.device, torch.float32).contiguous()
+        y = out if out is not None else torch.empty((x2.shape[0], self.rows), dtype=torch.float32, device=self.device)
+        check(lib().mv_q8_matvec_bf16(ctypes.byref(self._view), _p(x2), x2.shape[0], _p(s), _p(y),
+                                      self._tuning_ptr(tuning), _stream()))
+        return y[0] if x.dim() == 1 else y
+
+    def matvec_t_bf16(self, dy, scales, out=None, tuning=None):
+        """Transposed float form dx = W^T (scales * dy): dy bf16 [B, rows] -> fp32 [B, cols],
+        re-decoding the streams."""
+        d2 = dy.reshape(1, -1) if dy.dim() == 1 else dy
+        if d2.dtype != torch.bfloat16 or d2.shape[-1] != self.rows:
+            raise ValueError(f"dy must be bf16 with {self.rows} columns")
+        d2 = d2.to(self.device).contiguous()
+        s = scales.to(self.device, torch.float32).contiguous()
+        dx = out if out is not None else torch.empty((d2.shape[0], self.cols), dtype=torch.float32, device=self.device)
+        check(lib().mv_q8_matvec_t_bf16(ctypes.byref(self._view), _p(d2), d2.shape[0], _p(s), _p(dx),
+                                        self._tuning_ptr(tuning), _stream()))
+        return dx[0] if dy.dim() == 1 else dx
+
     def decode(self):
         W = torch.empty((self.rows, self.cols), dtype=torch.int8, device=self.device)
         check(lib().mv_q8_decode(ctypes.byref(self._view), _p(W), _stream()))
