@@ -366,6 +366,25 @@ def run_ours(args):
             del Ps, P
         torch.cuda.empty_cache()
 
+    # float form (configs[3] shapes): forward and re-decoding backward, us per call
+    float_form = {}
+    for m in mats:
+        if m["sigma"] != 4.0 or m["shape"] == (4096, 4096):
+            continue
+        rows, cols = m["shape"]
+        Mf = [e["M"] for e in entries if e["rows"] == rows and e["cols"] == cols and e["sigma"] == 4.0
+              and e["M"].local][0]
+        s_f = torch.from_numpy(np.random.default_rng(3).uniform(1e-3, 1e-2, rows).astype(np.float32)).to(dev)
+        for B in (1, 8, 64):
+            Xb = torch.randn((B, cols), device=dev).to(torch.bfloat16)
+            dYb = torch.randn((B, rows), device=dev).to(torch.bfloat16)
+            yf = torch.empty((B, rows), dtype=torch.float32, device=dev)
+            dxf = torch.empty((B, cols), dtype=torch.float32, device=dev)
+            tf, _ = time_graph(torch, lambda: Mf.matvec_bf16(Xb, s_f, out=yf), 10)
+            tb, _ = time_graph(torch, lambda: Mf.matvec_t_bf16(dYb, s_f, out=dxf), 10)
+            float_form[f"{rows}x{cols}_B{B}"] = {"fwd_us": 1e3 * tf, "bwd_us": 1e3 * tb, "bwd_over_fwd": tb / tf}
+    ops.device_status()
+
     # end to end through the public API: pinned host x in, int32 y out, every step
     xh = {c: torch.from_numpy(v).pin_memory() for c, v in x_by_cols.items()}
     yh = [torch.empty((1, e["rows"]), dtype=torch.int32).pin_memory() for e in entries]
@@ -415,6 +434,7 @@ def run_ours(args):
             "per_matrix": per,
             "dense_dp4a": dense, "cublas_sgemv_fp32": cublas, "ans_warp_rows_kernel": awr_t,
             "warp_per_row_kernel": wpr_t,
+            "float_form": float_form,
             "speedup_vs_dense_dp4a": {k: round(dense[k.split("_s")[0]]["us"] / v["us"], 3)
                                       for k, v in per.items() if k.split("_s")[0] in dense and "_s4_" in k},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
