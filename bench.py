@@ -224,15 +224,11 @@ def copies_for(nbytes):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
+    from matvans_b200 import dist as mvd
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = mvd.env_rank()
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    mvd.init("nccl", timeout_s=120, device=torch.device("cuda", local))
 
     from matvans_b200 import codec, ops
 
@@ -277,8 +273,7 @@ def run_ours(args):
             step()
         torch.cuda.synchronize()
         ops.device_status()
-        if world > 1:
-            dist.destroy_process_group()
+        mvd.shutdown()
         return 0
 
     for _ in range(max(args.warmup, 3)):
@@ -291,8 +286,7 @@ def run_ours(args):
 
     sampler = ClockSampler(local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
+    mvd.barrier()
     torch.cuda.synchronize()
     with sampler:
         e0.record()
@@ -300,15 +294,10 @@ def run_ours(args):
             g.replay()
         e1.record()
         torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    mvd.barrier()
     step_bytes = sum(int8_equiv_bytes(e["rows"], e["cols"]) for e in entries)
-    value = world * step_bytes / (ms * 1e-3) / 1e9
+    value, sec = mvd.aggregate_throughput(step_bytes / 1e9, e0.elapsed_time(e1) / args.steps * 1e-3, device=dev)
+    ms = sec * 1e3
     alg = sum(e["alg_bytes"] for e in entries)
     peak, peak_kind = measured_peak()
     achieved = alg / (ms * 1e-3) / 1e9
@@ -448,9 +437,8 @@ def run_ours(args):
             "cpu_baseline": cb,
         }
     del g
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    mvd.barrier()
+    mvd.shutdown()
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0

@@ -368,7 +368,6 @@ struct BwdCons {
         float w[4];
         i8x4_to_f32(wq, w);
         const bool b4 = lane & 16, b3 = lane & 8;
-        const int col = 4 * q + (b4 ? 2 : 0) + (b3 ? 1 : 0);
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             const float a0 = w[0] * g[v], a1 = w[1] * g[v], a2 = w[2] * g[v], a3 = w[3] * g[v];
@@ -382,7 +381,21 @@ struct BwdCons {
             k += __shfl_xor_sync(0xffffffffu, k, 4);
             k += __shfl_xor_sync(0xffffffffu, k, 2);
             k += __shfl_xor_sync(0xffffffffu, k, 1);
-            if ((lane & 7) == 0 && col < cols) atomicAdd(dx + (size_t)v * cols + col, k);
+            // column 4q + j sits in lane 8*(2*(j>>1) + (j&1)) = lanes 0, 8, 16, 24: one
+            // 16-byte vector reduction from lane 0 instead of four scalar atomics
+            const float c1 = __shfl_sync(0xffffffffu, k, 8), c2 = __shfl_sync(0xffffffffu, k, 16);
+            const float c3 = __shfl_sync(0xffffffffu, k, 24);
+            if (lane == 0) {
+                float *dst = dx + (size_t)v * cols + 4 * q;
+                if (4 * q + 3 < cols) {
+                    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(k), "f"(c1), "f"(c2),
+                                 "f"(c3)
+                                 : "memory");
+                } else {
+                    const float c[4] = {k, c1, c2, c3};
+                    for (int jj = 0; jj < 4 && 4 * q + jj < cols; jj++) atomicAdd(dst + jj, c[jj]);
+                }
+            }
         }
     }
     __device__ __forceinline__ void use(const Group &, int, int q, uint32_t wq, int lane) { scatter(q, wq, lane); }
