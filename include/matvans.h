@@ -177,9 +177,14 @@ mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int3
  *   ctas_per_sm  cap on resident CTAs per SM (default: occupancy limit)
  *   parts        work items per 32-row stripe (its segments split in `parts`
  *                ranges; default: whole stripes in stacks, enough parts to
- *                fill the GPU for a single matrix) */
+ *                fill the GPU for a single matrix)
+ *   engine       int8 product of 8..16 vectors: 0 = tensor cores
+ *                (tcgen05.mma kind::i8, TMEM accumulators; ilp is then 1),
+ *                1 = CUDA cores (dp4a).  Fewer vectors always use dp4a. */
+#define MV_ENGINE_AUTO 0
+#define MV_ENGINE_DP4A 1
 typedef struct mv_q8_tuning {
-    int32_t warps, ilp, depth, ctas_per_sm, parts;
+    int32_t warps, ilp, depth, ctas_per_sm, parts, engine;
 } mv_q8_tuning;
 
 /* mv_q8_matvec with explicit launch parameters (needs cols % 16 == 0,

@@ -46,7 +46,7 @@ class Q8View(ctypes.Structure):
 class Q8Tuning(ctypes.Structure):
     """struct mv_q8_tuning."""
     _fields_ = [("warps", ctypes.c_int32), ("ilp", ctypes.c_int32), ("depth", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("parts", ctypes.c_int32)]
+                ("ctas_per_sm", ctypes.c_int32), ("parts", ctypes.c_int32), ("engine", ctypes.c_int32)]
 
 
 class Q8Job(ctypes.Structure):

@@ -22,10 +22,20 @@ import torch
 from . import _lib
 from ._lib import Q8Tuning
 
-CANDIDATES = [(w, ilp, d, 0, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)]
+# (warps, ilp, depth, ctas_per_sm, parts, engine)
+CANDIDATES = [(w, ilp, d, 0, 0, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)]
 # single matrices additionally try splitting each stripe into more work items
-SINGLE_CANDIDATES = CANDIDATES + [(w, ilp, d, 0, p) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)
+SINGLE_CANDIDATES = CANDIDATES + [(w, ilp, d, 0, p, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)
                                   for p in (2, 4)]
+
+
+def candidates_for(batch, base):
+    """Candidates at `batch` vectors: 8..16 vectors run on the tensor cores
+    (engine 0, where ilp is fixed at 1) or on the CUDA cores (engine 1)."""
+    if batch < 8:
+        return list(base)
+    mma = [c for c in base if c[1] == 1]
+    return mma + [c[:5] + (1,) for c in base]
 L2_BYTES = 126 * 2 ** 20
 _lock = threading.Lock()
 
@@ -97,8 +107,10 @@ def time_launches(fns, reps=10):
     return e0.elapsed_time(e1) / reps / len(fns)
 
 
-def tune(M, batch=1, candidates=SINGLE_CANDIDATES, reps=10, force=False):
+def tune(M, batch=1, candidates=None, reps=10, force=False):
     """Best Q8Tuning for matrix M at `batch` vectors (cached)."""
+    if candidates is None:
+        candidates = candidates_for(batch, SINGLE_CANDIDATES)
     k = key(M, batch)
     with _lock:
         db = _load()

@@ -32,6 +32,7 @@
 #include <cstdio>
 
 #include "mv_device.cuh"
+#include "umma.cuh"
 
 namespace mv {
 
@@ -209,6 +210,14 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
 template <int NV>
 struct IntCons {
     static constexpr int kNV = NV;
+    static constexpr int kTmemCols = 0;
+    static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
+    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
+    __device__ __forceinline__ void drain(const Q8SLaunch &) {}
+    template <int ILP>
+    __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
+                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
+                                             int lane);
     const int8_t *x;
     int cols;
     int acc[NV];
@@ -272,6 +281,14 @@ __device__ __forceinline__ float bf16_hi(uint32_t u) { return __uint_as_float(u 
 template <int NV>
 struct FwdCons {
     static constexpr int kNV = NV;
+    static constexpr int kTmemCols = 0;
+    static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
+    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
+    __device__ __forceinline__ void drain(const Q8SLaunch &) {}
+    template <int ILP>
+    __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
+                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
+                                             int lane);
     const uint16_t *x;
     int cols;
     float acc[NV];
@@ -346,6 +363,14 @@ struct FwdCons {
 template <int NV>
 struct BwdCons {
     static constexpr int kNV = NV;
+    static constexpr int kTmemCols = 0;
+    static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
+    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
+    __device__ __forceinline__ void drain(const Q8SLaunch &) {}
+    template <int ILP>
+    __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
+                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
+                                             int lane);
     float g[NV];
     float *dx;
     int cols;
@@ -455,6 +480,188 @@ __device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view
     if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
 }
 
+template <int NV>
+template <int ILP>
+__device__ __forceinline__ void IntCons<NV>::run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
+                                                      const uint32_t (&rows_now)[ILP], uint32_t *sb,
+                                                      const uint32_t *lut_l, int lane) {
+    decode_step<IntCons<NV>, ILP>(L, m, seg0, W, rows_now, sb, lut_l, lane, *this);
+}
+template <int NV>
+template <int ILP>
+__device__ __forceinline__ void FwdCons<NV>::run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
+                                                      const uint32_t (&rows_now)[ILP], uint32_t *sb,
+                                                      const uint32_t *lut_l, int lane) {
+    decode_step<FwdCons<NV>, ILP>(L, m, seg0, W, rows_now, sb, lut_l, lane, *this);
+}
+template <int NV>
+template <int ILP>
+__device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
+                                                      const uint32_t (&rows_now)[ILP], uint32_t *sb,
+                                                      const uint32_t *lut_l, int lane) {
+    decode_step<BwdCons<NV>, ILP>(L, m, seg0, W, rows_now, sb, lut_l, lane, *this);
+}
+
+// y = W x for 8..16 int8 vectors on the tensor cores.  Every 8 decoded quads
+// the 32 lanes of a warp (= the 32 rows of the stripe) hold a 32 x 32 int8
+// tile of W; it is written to shared memory in the canonical K-major layout
+// (8-row x 16-byte core matrices, LBO 128 B, SBO 256 B) and one lane issues
+// tcgen05.mma.kind::i8 with M = 128 (A = the x tile; only the rows of this
+// warp's TMEM lane quarter hold the real vectors, the others are ignored),
+// N = 32 (B = the W tile), K = 32, accumulating exactly in int32 in the warp's
+// own 32 TMEM columns.  W tiles are double-buffered; a tcgen05.commit to an
+// mbarrier tells when a tile may be overwritten.  ILP 1 only.
+struct MmaCons {
+    static constexpr int kNV = 16;
+    static constexpr int kTmemCols = 1;  // > 0: the kernel allocates TMEM
+    static constexpr int kXChunks = 8;   // x tile: 8 chunks of 32 columns x 16 vectors (512 B each)
+    static __host__ __device__ constexpr size_t extra_bytes(int W) {
+        // x tile 4 KB + W tiles 2 x 1 KB per warp, 2 mbarriers per warp, TMEM address slot
+        return (size_t)W * (kXChunks * 512 + 2048) + (size_t)W * 16 + 128;
+    }
+    static __host__ __device__ constexpr uint32_t tmem_cols(int W) {
+        return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : 256;
+    }
+    uint32_t xt, wt0, wt1, d_tmem, ld_addr, nc0, nc1, wsel, warp_q;
+    uint64_t *mbar;
+    const int8_t *x;
+    int cols, batch;
+    bool any;
+
+    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int warp,
+                                         int lane, int W) {
+        const uint32_t base = smem_u32(extra);
+        xt = base + (uint32_t)warp * 4096u;
+        wt0 = base + (uint32_t)W * 4096u + (uint32_t)warp * 2048u;
+        wt1 = wt0 + 1024u;
+        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 6144) + 2 * warp;
+        if (lane == 0) {
+            mbar_init(&mbar[0], 1);
+            mbar_init(&mbar[1], 1);
+        }
+        fence_mbar_init();
+        __syncwarp();
+        d_tmem = tmem_base + 32u * (uint32_t)warp;
+        warp_q = (uint32_t)(warp & 3);
+        ld_addr = tmem_base + ((32u * warp_q) << 16) + 32u * (uint32_t)warp;
+        nc0 = nc1 = wsel = 0;
+    }
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
+        x = J.x;
+        cols = J.m.cols;
+        batch = L.batch;
+        any = false;
+    }
+    // wait until the MMA that last read W-tile buffer t (and all earlier ones) completed
+    __device__ __forceinline__ bool wait_buf(const Q8SLaunch &L, int t) {
+        const uint32_t n = t ? nc1 : nc0;
+        if (n == 0) return true;
+        return mbar_wait_bounded(&mbar[t], (n - 1) & 1, L.status, L.spin_limit);
+    }
+    __device__ __forceinline__ bool wait_all(const Q8SLaunch &L) {
+        // the most recent commit covers every earlier MMA of this thread
+        const int last = wsel ^ 1;
+        return wait_buf(L, last) && wait_buf(L, last ^ 1);
+    }
+    template <int ILP>
+    __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int,
+                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
+                                             int lane) {
+        const int qtot = (m.cols + 3) >> 2;
+        const int q0 = seg0 * m.seg_quads;
+        const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
+        if (nq <= 0) return;
+        const int nchunks = (nq + 7) >> 3;
+        uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
+        const uint32_t kend = rows_now[0] * 32 + lane;
+        // x is staged in windows of at most kXChunks chunks (the per-warp x tile)
+        for (int c0 = 0; c0 < nchunks; c0 += kXChunks) {
+            const int cn = min(kXChunks, nchunks - c0);
+            wait_all(L);  // every earlier MMA has read the previous window
+            for (int p = lane; p < 32 * cn; p += 32) {
+                const int c = p >> 5, b = (p & 31) >> 1, h = p & 1;
+                const int col = 4 * q0 + 32 * (c0 + c) + 16 * h;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (b < batch && col < cols) v = __ldg(reinterpret_cast<const uint4 *>(x + (size_t)b * cols + col));
+                const uint32_t dst = xt + (uint32_t)c * 512u + (uint32_t)(b >> 3) * 256u + (uint32_t)h * 128u +
+                                     (uint32_t)(b & 7) * 16u;
+                asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst), "r"(v.x), "r"(v.y), "r"(v.z),
+                             "r"(v.w)
+                             : "memory");
+            }
+            for (int c = 0; c < cn; c++) {
+                const int qc = 8 * (c0 + c);
+                uint32_t w[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
+                const int t = (int)wsel;
+                wsel ^= 1;
+                wait_buf(L, t);
+                const uint32_t tile = t ? wt1 : wt0;
+                const uint32_t dst = tile + (uint32_t)(lane >> 3) * 256u + (uint32_t)(lane & 7) * 16u;
+                asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst), "r"(w[0]), "r"(w[1]), "r"(w[2]),
+                             "r"(w[3])
+                             : "memory");
+                asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst + 128u), "r"(w[4]), "r"(w[5]),
+                             "r"(w[6]), "r"(w[7])
+                             : "memory");
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    tcgen05_fence_after();
+                    const uint64_t a = umma_smem_desc(xt + (uint32_t)c * 512u - warp_q * 1024u, 128u, 256u);
+                    const uint64_t bdesc = umma_smem_desc(tile, 128u, 256u);
+                    umma_i8(d_tmem, a, bdesc, umma_idesc_i8(128, 32), any ? 1u : 0u);
+                    umma_commit(&mbar[t]);
+                }
+                __syncwarp();
+                any = true;
+                if (t) nc1++;
+                else nc0++;
+            }
+        }
+        if (nq > 0 && (hi != 0 || lo != P)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+    }
+    __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
+                                                int W, void *red_smem) {
+        int *red = reinterpret_cast<int *>(red_smem);  // [W][32 rows][16 vectors]
+        uint32_t r[32];
+        if (any) {
+            wait_all(L);
+            tcgen05_fence_after();
+            tmem_ld_32x32b_x32(ld_addr, r);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; j++) r[j] = 0;
+        }
+        if (lane < 16) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) red[(warp * 32 + j) * 16 + lane] = (int)r[j];
+        }
+        tcgen05_fence_before();
+        __syncthreads();
+        const mv_q8_view &m = J.m;
+        for (int t = threadIdx.x; t < 16 * 32; t += blockDim.x) {
+            const int v = t >> 5, l = t & 31;
+            int sum = 0;
+            for (int w = 0; w < W; w++) sum += red[(w * 32 + l) * 16 + v];
+            const int row = stripe * 32 + l;
+            if (row < m.rows && v < L.batch) {
+                int32_t *dst = J.y + (size_t)v * m.rows + row;
+                if (J.atomic) {
+                    atomicAdd(dst, sum);
+                } else {
+                    *dst = sum;
+                    if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_all(L); }
+};
+
 template <class Cons, int ILP, int DEPTH>
 __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
     constexpr int NV = Cons::kNV;
@@ -463,7 +670,8 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
     const int W = blockDim.x >> 5;
 
     uint32_t *lut = reinterpret_cast<uint32_t *>(smem);                                 // 8192 words
-    uint32_t *bufs = lut + 256 * 32;                                                     // [W][DEPTH][ILP][buf]
+    unsigned char *extra = smem + 256 * 32 * 4;                                          // consumer region
+    uint32_t *bufs = reinterpret_cast<uint32_t *>(extra + Cons::extra_bytes(W));         // [W][DEPTH][ILP][buf]
     int *red = reinterpret_cast<int *>(bufs + (size_t)W * DEPTH * ILP * L.buf_words);    // [W][NV][32]
     uint64_t *bars = reinterpret_cast<uint64_t *>(red + W * NV * 32);                    // [W][DEPTH]
     uint32_t *toff_s = reinterpret_cast<uint32_t *>(bars + W * DEPTH);                   // [36]
@@ -473,6 +681,19 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
     uint32_t *my_bufs = bufs + (size_t)warp * DEPTH * ILP * L.buf_words;
     uint32_t *my_rows = rows_s + warp * DEPTH * ILP;
     uint64_t *my_bars = bars + warp * DEPTH;
+
+    // tensor-memory accumulators (MMA consumers): one warp allocates, all use, it frees at the end
+    uint32_t tmem_base = 0;
+    if (Cons::kTmemCols) {
+        uint32_t *slot = reinterpret_cast<uint32_t *>(extra + Cons::extra_bytes(W) - 128);
+        if (warp == 0) tmem_alloc(slot, MmaCons::tmem_cols(W));
+        tcgen05_fence_before();
+        __syncthreads();
+        tcgen05_fence_after();
+        tmem_base = *slot;
+    }
+    Cons cons;
+    cons.init(L, extra, tmem_base, warp, lane, W);
     if (lane == 0)
         for (int d = 0; d < DEPTH; d++) mbar_init(&my_bars[d], 1);
     fence_mbar_init();
@@ -538,7 +759,6 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
             lut_stripe = I.stripe;
         }
 
-        Cons cons;
         cons.begin_item(L, J, I.stripe, lane);
         const int steps = warp_steps(send - sbeg, warp, W, ILP);
         for (int j = 0; j < steps; j++) {
@@ -553,8 +773,8 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
             }
             if (any) {
                 if (mbar_wait_bounded(&my_bars[slot], parity, L.status, L.spin_limit)) {
-                    decode_step<Cons, ILP>(L, m, sbeg + warp + j * W * ILP, W, rows_now,
-                                           my_bufs + slot * ILP * L.buf_words, lut_l, lane, cons);
+                    cons.template run_step<ILP>(L, m, sbeg + warp + j * W * ILP, W, rows_now,
+                                                my_bufs + slot * ILP * L.buf_words, lut_l, lane);
                 } else {
                     mbar_wait_bounded(&my_bars[slot], parity, nullptr, L.spin_limit);
                 }
@@ -572,6 +792,12 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
         }
 
         cons.finish_item(L, J, I.stripe, warp, lane, W, red);
+    }
+    if (Cons::kTmemCols) {
+        cons.drain(L);
+        tcgen05_fence_before();
+        __syncthreads();
+        if (warp == 0) tmem_dealloc(tmem_base, MmaCons::tmem_cols(W));
     }
 }
 
@@ -601,14 +827,14 @@ __global__ void q8s_scale_atomic_y(const Q8Job *jobs, int njobs, int batch) {
 
 namespace {
 
-size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage) {
-    return 256 * 32 * 4 + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 + (size_t)W * DEPTH * 8 +
+size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage, size_t extra) {
+    return 256 * 32 * 4 + extra + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 + (size_t)W * DEPTH * 8 +
            36 * 4 + (size_t)W * DEPTH * ILP * 4 + (size_t)tbl_stage * 2;
 }
 
 template <class Cons, int ILP, int DEPTH>
 mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t st) {
-    const size_t smem = q8s_smem(Cons::kNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage);
+    const size_t smem = q8s_smem(Cons::kNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage, Cons::extra_bytes(W));
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch needs %zu B of shared memory (max %d)", smem,
                     max_smem_optin());
@@ -617,6 +843,7 @@ mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t 
     mv_status rc = prepare_kernel((const void *)kern, smem, 32 * W, &bps);
     if (rc) return rc;
     if (ctas_per_sm > 0) bps = std::min(bps, ctas_per_sm);
+    if (Cons::kTmemCols) bps = std::max(1, std::min<int>(bps, 512 / MmaCons::tmem_cols(W)));
     const long long grid = std::max(1LL, std::min<long long>(L.nitems, (long long)bps * sm_count()));
     kern<<<(unsigned)grid, 32 * W, smem, st>>>(L);
     MV_CUDA_TRY(cudaGetLastError(), "q8 stack kernel launch");
@@ -625,15 +852,21 @@ mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t 
 
 template <class Cons>
 mv_status launch_q8s_c(const Q8SLaunch &L, const mv_q8_tuning &t, cudaStream_t st) {
-    if (t.ilp == 2) {
-        if (t.depth == 2) return launch_q8s_t<Cons, 2, 2>(L, t.warps, t.ctas_per_sm, st);
-        return launch_q8s_t<Cons, 2, 1>(L, t.warps, t.ctas_per_sm, st);
+    if constexpr (Cons::kTmemCols != 0) {  // the MMA consumer decodes one segment per warp step
+        if (t.depth == 2) return launch_q8s_t<Cons, 1, 2>(L, t.warps, t.ctas_per_sm, st);
+        return launch_q8s_t<Cons, 1, 1>(L, t.warps, t.ctas_per_sm, st);
+    } else {
+        if (t.ilp == 2) {
+            if (t.depth == 2) return launch_q8s_t<Cons, 2, 2>(L, t.warps, t.ctas_per_sm, st);
+            return launch_q8s_t<Cons, 2, 1>(L, t.warps, t.ctas_per_sm, st);
+        }
+        if (t.depth == 2) return launch_q8s_t<Cons, 1, 2>(L, t.warps, t.ctas_per_sm, st);
+        return launch_q8s_t<Cons, 1, 1>(L, t.warps, t.ctas_per_sm, st);
     }
-    if (t.depth == 2) return launch_q8s_t<Cons, 1, 2>(L, t.warps, t.ctas_per_sm, st);
-    return launch_q8s_t<Cons, 1, 1>(L, t.warps, t.ctas_per_sm, st);
 }
 
 mv_status launch_q8s(const Q8SLaunch &L, int nv, const mv_q8_tuning &t, cudaStream_t st) {
+    if (nv >= 8 && t.engine == MV_ENGINE_AUTO) return launch_q8s_c<MmaCons>(L, t, st);
     switch (nv) {
         case 1: return launch_q8s_c<IntCons<1>>(L, t, st);
         case 2: return launch_q8s_c<IntCons<2>>(L, t, st);
@@ -664,8 +897,9 @@ mv_status launch_q8f(const Q8SLaunch &L, int mode, int nv, const mv_q8_tuning &t
 int nv_round(int nb) { return nb <= 2 ? nb : nb <= 4 ? 4 : nb <= 8 ? 8 : 16; }
 
 mv_q8_tuning resolve(const mv_q8_tuning *t) {
-    mv_q8_tuning r{8, 2, 1, 0, 0};
+    mv_q8_tuning r{8, 2, 1, 0, 0, MV_ENGINE_AUTO};
     if (t) {
+        if (t->engine == MV_ENGINE_DP4A) r.engine = MV_ENGINE_DP4A;
         if (t->parts > 0) r.parts = t->parts;
         if (t->warps > 0) r.warps = std::min(8, t->warps);
         if (t->ilp == 1 || t->ilp == 2) r.ilp = t->ilp;
