@@ -194,6 +194,120 @@ def run_reference(args):
     return 0
 
 
+# ------------------------------------------------------------------ batched stack (224 matrices)
+
+LAYER = [("q", 4096, 4096), ("k", 4096, 4096), ("v", 4096, 4096), ("o", 4096, 4096),
+         ("gate", 11008, 4096), ("up", 11008, 4096), ("down", 4096, 11008)]
+
+
+def stack_specs(layers=32, seed=20251204):
+    """7 matrices per layer; each with its own sigma ~ U[2,6]; 10% of them
+    Laplace(b=3) with 0.1% outliers at +-100 instead."""
+    rng = np.random.default_rng(seed)
+    n = layers * len(LAYER)
+    lap = set(rng.choice(n, size=int(round(0.1 * n)), replace=False).tolist())
+    specs = []
+    for i in range(n):
+        name, r, c = LAYER[i % len(LAYER)]
+        specs.append(dict(name=f"L{i // len(LAYER)}.{name}", rows=r, cols=c, sigma=float(rng.uniform(2, 6)),
+                          laplace=i in lap, seed=seed + 1 + i))
+    return specs
+
+
+def gen_on_device(torch, spec, dev):
+    """Seeded int8 weights generated on the GPU (host numpy generation of 6.5 G weights takes minutes)."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(spec["seed"])
+    shape = (spec["rows"], spec["cols"])
+    if spec["laplace"]:
+        e1 = torch.empty(shape, device=dev).exponential_(generator=g)
+        e2 = torch.empty(shape, device=dev).exponential_(generator=g)
+        z = 3.0 * (e1 - e2)
+        del e1, e2
+        u = torch.rand(shape, device=dev, generator=g)
+        z = torch.where(u < 0.0005, torch.full_like(z, -100.0), torch.where(u < 0.001, torch.full_like(z, 100.0), z))
+        del u
+    else:
+        z = torch.randn(shape, device=dev, generator=g) * spec["sigma"]
+    return torch.clamp(torch.round(z), -127, 127).to(torch.int8)
+
+
+def entropy_dev(torch, Wd):
+    cnt = torch.bincount((Wd.reshape(-1).to(torch.int32) + 128), minlength=256).double()
+    p = cnt[cnt > 0] / cnt.sum()
+    return float(-(p * torch.log2(p)).sum())
+
+
+def build_stack(torch, ops, dev, layers=32, keep_dense=True):
+    from matvans_b200 import codec
+    mats = []
+    for sp in stack_specs(layers):
+        Wd = gen_on_device(torch, sp, dev)
+        M = ops.Q8Matrix(codec.q8_encode(Wd.cpu().numpy(), local=True), dev)
+        mats.append(dict(spec=sp, M=M, Wd=Wd if keep_dense else None, entropy=entropy_dev(torch, Wd)))
+    return mats
+
+
+def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, reps=10):
+    """configs: the 224-matrix uneven stack, one persistent launch per step, B in {1,4,8,16}; the tensor-core
+    engine competes with dp4a at B >= 8.  Gate: bit-exact against the dense int8 kernel on the same x."""
+    t_build = time.perf_counter()
+    mats = build_stack(torch, ops, dev, layers)
+    t_build = time.perf_counter() - t_build
+    Ms = [m["M"] for m in mats]
+    weights = sum(M.rows * M.cols for M in Ms)
+    comp = sum(M.payload_bytes for M in Ms)
+    out = {"matrices": len(Ms), "weights": weights, "compressed_bytes": comp,
+           "bits_per_weight": 8.0 * comp / weights,
+           "entropy_bits_mean": float(np.mean([m["entropy"] for m in mats])),
+           "laplace_matrices": sum(m["spec"]["laplace"] for m in mats), "build_s": round(t_build, 1), "batches": {}}
+    g = torch.Generator(device=dev)
+    g.manual_seed(99)
+    for B in batches:
+        xs = [torch.randint(-127, 128, (B, M.cols), dtype=torch.int8, device=dev, generator=g) for M in Ms]
+        ref = [torch.empty((B, M.rows), dtype=torch.int32, device=dev) for M in Ms]
+
+        def dense_step():
+            for m, x, y in zip(mats, xs, ref):
+                ops.dense_matvec(m["Wd"], x, out=y)
+
+        t_dense, gd = time_graph(torch, dense_step, reps)
+        del gd
+        cands = autotune.candidates_for(B, autotune.CANDIDATES)
+        best, res = autotune.tune_stack(lambda t: ops.Q8Stack(Ms, batch=B, tuning=t, xs=xs, device=dev),
+                                        candidates=cands, reps=reps)
+        row = {}
+        engines = (0, 1) if B >= 8 else (0,)
+        for eng in engines:
+            mine = {k: v for k, v in res.items() if int(k.split(",")[5]) == eng}
+            if not mine:
+                continue
+            kbest = min(mine, key=mine.get)
+            S = ops.Q8Stack(Ms, batch=B, tuning=tuple(int(v) for v in kbest.split(",")), xs=xs, device=dev)
+            S.run()
+            torch.cuda.synchronize()
+            for y, yr, m in zip(S.ys, ref, mats):
+                if not torch.equal(y, yr):
+                    raise SystemExit(f"bench: stack {m['spec']['name']} B={B} engine {eng} is not bit-exact")
+            t_ms, gs = time_graph(torch, S.run, reps)
+            del gs, S
+            name = "tcgen05" if (eng == 0 and B >= 8) else "dp4a"
+            row[name] = {"us_per_step": round(1e3 * t_ms, 1), "tuning": kbest,
+                         "int8_equiv_gbs": round(sum(int8_equiv_bytes(M.rows, M.cols, B) for M in Ms) / t_ms / 1e6, 1),
+                         "compressed_gbs": round(comp / t_ms / 1e6, 1),
+                         "us_per_matvec": round(1e3 * t_ms / len(Ms), 3)}
+        fastest = min(row.values(), key=lambda v: v["us_per_step"])
+        row["candidates_us"] = {k: round(v, 1) for k, v in sorted(res.items(), key=lambda kv: kv[1])}
+        row["dense_dp4a_us_per_step"] = round(1e3 * t_dense, 1)
+        row["speedup_vs_dense_dp4a"] = round(1e3 * t_dense / fastest["us_per_step"], 3)
+        out["batches"][f"B{B}"] = row
+        del xs, ref
+    del mats, Ms
+    torch.cuda.empty_cache()
+    ops.device_status()
+    return out
+
+
 # ------------------------------------------------------------------ GPU arm
 
 def time_graph(torch, fn, reps, inner=1):
@@ -374,6 +488,8 @@ def run_ours(args):
             float_form[f"{rows}x{cols}_B{B}"] = {"fwd_us": 1e3 * tf, "bwd_us": 1e3 * tb, "bwd_over_fwd": tb / tf}
     ops.device_status()
 
+    stack224 = None if args.no_stack else stack_section(torch, ops, autotune, dev)
+
     # end to end through the public API: pinned host x in, int32 y out, every step
     xh = {c: torch.from_numpy(v).pin_memory() for c, v in x_by_cols.items()}
     yh = [torch.empty((1, e["rows"]), dtype=torch.int32).pin_memory() for e in entries]
@@ -424,6 +540,7 @@ def run_ours(args):
             "dense_dp4a": dense, "cublas_sgemv_fp32": cublas, "ans_warp_rows_kernel": awr_t,
             "warp_per_row_kernel": wpr_t,
             "float_form": float_form,
+            "stack224": stack224,
             "speedup_vs_dense_dp4a": {k: round(dense[k.split("_s")[0]]["us"] / v["us"], 3)
                                       for k, v in per.items() if k.split("_s")[0] in dense and "_s4_" in k},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -444,6 +561,29 @@ def run_ours(args):
     return 0
 
 
+def run_profile_stack(args):
+    """Small fixed stack case for ncu: gate + two plain steps."""
+    import torch
+    from matvans_b200 import ops
+    layers, B, engine = (int(v) for v in args.profile_stack.split(","))
+    dev = torch.device("cuda", 0)
+    mats = build_stack(torch, ops, dev, layers)
+    Ms = [m["M"] for m in mats]
+    g = torch.Generator(device=dev)
+    g.manual_seed(99)
+    xs = [torch.randint(-127, 128, (B, M.cols), dtype=torch.int8, device=dev, generator=g) for M in Ms]
+    S = ops.Q8Stack(Ms, batch=B, tuning=(4, 1, 1, 0, 0, engine), xs=xs, device=dev)
+    S.run()
+    for m, x, y in zip(mats, xs, S.ys):
+        if not torch.equal(y, ops.dense_matvec(m["Wd"], x)):
+            raise SystemExit(f"bench: {m['spec']['name']} is not bit-exact")
+    for _ in range(2):
+        S.run()
+    torch.cuda.synchronize()
+    ops.device_status()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -451,6 +591,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-stack", action="store_true", help="skip the 224-matrix batched stack section")
+    ap.add_argument("--profile-stack", default="",
+                    help="LAYERS,B,ENGINE: build a stack of LAYERS x 7 matrices and run two steps at B vectors "
+                         "with the given engine (the case ncu captures)")
     ap.add_argument("--tuning", default="", help="fixed stack launch parameters warps,ilp,depth,ctas_per_sm "
                                                   "(default: autotuned)")
     ap.add_argument("--profile", action="store_true",
@@ -458,6 +602,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_stack:
+        return run_profile_stack(args)
     return run_ours(args)
 
 

@@ -210,8 +210,11 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
 template <int NV>
 struct IntCons {
     static constexpr int kNV = NV;
+    static constexpr int kRedNV = NV;
+    static constexpr int kMinCtas = 1;
     static constexpr int kTmemCols = 0;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
     __device__ __forceinline__ void drain(const Q8SLaunch &) {}
     template <int ILP>
@@ -281,8 +284,11 @@ __device__ __forceinline__ float bf16_hi(uint32_t u) { return __uint_as_float(u 
 template <int NV>
 struct FwdCons {
     static constexpr int kNV = NV;
+    static constexpr int kRedNV = NV;
+    static constexpr int kMinCtas = 1;
     static constexpr int kTmemCols = 0;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
     __device__ __forceinline__ void drain(const Q8SLaunch &) {}
     template <int ILP>
@@ -363,8 +369,11 @@ struct FwdCons {
 template <int NV>
 struct BwdCons {
     static constexpr int kNV = NV;
+    static constexpr int kRedNV = NV;
+    static constexpr int kMinCtas = 1;
     static constexpr int kTmemCols = 0;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
     __device__ __forceinline__ void drain(const Q8SLaunch &) {}
     template <int ILP>
@@ -510,20 +519,35 @@ __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const 
 // warp's TMEM lane quarter hold the real vectors, the others are ignored),
 // N = 32 (B = the W tile), K = 32, accumulating exactly in int32 in the warp's
 // own 32 TMEM columns.  W tiles are double-buffered; a tcgen05.commit to an
-// mbarrier tells when a tile may be overwritten.  ILP 1 only.
+// mbarrier tells when a tile may be overwritten.  x moves through a 4-chunk
+// window (4 x 32 columns x 16 vectors); the next window is loaded into
+// registers while the current one is in use.  Shared memory per warp is kept
+// small so that 12-16 warps fit on an SM: the x tiles double as the
+// cross-warp reduction area and as the staging area of the decode tables.
+// ILP 1 only.
 struct MmaCons {
     static constexpr int kNV = 16;
-    static constexpr int kTmemCols = 1;  // > 0: the kernel allocates TMEM
-    static constexpr int kXChunks = 8;   // x tile: 8 chunks of 32 columns x 16 vectors (512 B each)
+    static constexpr int kRedNV = 0;      // reduction area: the x tiles
+    static constexpr int kMinCtas = 2;    // 2 x 8 warps per SM: at most 128 registers per thread
+    static constexpr int kTmemCols = 1;   // > 0: the kernel allocates TMEM
+    static constexpr int kXChunks = 4;    // x tile: 4 chunks of 32 columns x 16 vectors (512 B each)
+    static constexpr int kXBytes = kXChunks * 512;
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
-        // x tile 4 KB + W tiles 2 x 1 KB per warp, 2 mbarriers per warp, TMEM address slot
-        return (size_t)W * (kXChunks * 512 + 2048) + (size_t)W * 16 + 128;
+        // x tile 2 KB + W tiles 2 x 1 KB per warp, 2 mbarriers per warp, TMEM address slot; at least the
+        // span an A operand reads (16 row groups of 256 B from the last chunk of the last x tile), so that
+        // the ignored rows never reach past this region
+        return std::max<size_t>((size_t)W * (kXBytes + 2048) + (size_t)W * 16 + 128,
+                                (size_t)(W - 1) * kXBytes + (kXChunks - 1) * 512 + 16 * 256 + 128);
     }
+    // the decode tables are staged in the x tiles when they fit
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)W * kXBytes; }
     static __host__ __device__ constexpr uint32_t tmem_cols(int W) {
-        return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : 256;
+        return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : W <= 8 ? 256 : 512;
     }
-    uint32_t xt, wt0, wt1, d_tmem, ld_addr, nc0, nc1, wsel, warp_q;
+    uint32_t xt, wt0, d_tmem, ld_addr, nc0, nc1, wsel;
+    uint64_t a_desc0, b_desc0;
     uint64_t *mbar;
+    int *xbase;
     const int8_t *x;
     int cols, batch;
     bool any;
@@ -531,19 +555,23 @@ struct MmaCons {
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int warp,
                                          int lane, int W) {
         const uint32_t base = smem_u32(extra);
-        xt = base + (uint32_t)warp * 4096u;
-        wt0 = base + (uint32_t)W * 4096u + (uint32_t)warp * 2048u;
-        wt1 = wt0 + 1024u;
-        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 6144) + 2 * warp;
+        xbase = reinterpret_cast<int *>(extra);
+        xt = base + (uint32_t)warp * (uint32_t)kXBytes;
+        wt0 = base + (uint32_t)W * (uint32_t)kXBytes + (uint32_t)warp * 2048u;
+        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * (kXBytes + 2048)) + 2 * warp;
         if (lane == 0) {
             mbar_init(&mbar[0], 1);
             mbar_init(&mbar[1], 1);
         }
         fence_mbar_init();
         __syncwarp();
+        const uint32_t warp_q = (uint32_t)(warp & 3);
         d_tmem = tmem_base + 32u * (uint32_t)warp;
-        warp_q = (uint32_t)(warp & 3);
         ld_addr = tmem_base + ((32u * warp_q) << 16) + 32u * (uint32_t)warp;
+        // A starts 4 * warp_q row groups (1 KB each) before the x tile, so vector b lands in TMEM lane
+        // 32 * warp_q + b; the x tiles follow the 32 KB decode table, so the start stays in shared memory
+        a_desc0 = umma_smem_desc(xt - warp_q * 1024u, 128u, 256u);
+        b_desc0 = umma_smem_desc(wt0, 128u, 256u);
         nc0 = nc1 = wsel = 0;
     }
     __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
@@ -563,6 +591,42 @@ struct MmaCons {
         const int last = wsel ^ 1;
         return wait_buf(L, last) && wait_buf(L, last ^ 1);
     }
+    __device__ __forceinline__ void put_tile_and_mma(const Q8SLaunch &L, const uint32_t (&w)[8], int c, int lane,
+                                                     bool waited) {
+        const int t = (int)wsel;
+        if (!waited) wait_buf(L, t);
+        wsel ^= 1;
+        const uint32_t dst = wt0 + (uint32_t)t * 1024u + (uint32_t)(lane >> 3) * 256u + (uint32_t)(lane & 7) * 16u;
+        asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst), "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3])
+                     : "memory");
+        asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst + 128u), "r"(w[4]), "r"(w[5]), "r"(w[6]),
+                     "r"(w[7])
+                     : "memory");
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+            tcgen05_fence_after();
+            // descriptor start addresses are in 16-byte units: chunk c of the x tile is 512 B in, tile t 1 KB
+            umma_i8(d_tmem, a_desc0 + (uint64_t)(c * 32), b_desc0 + (uint64_t)(t * 64), umma_idesc_i8(128, 32),
+                    any ? 1u : 0u);
+            umma_commit(&mbar[t]);
+        }
+        any = true;
+        if (t) nc1++;
+        else nc0++;
+    }
+    // lane (b, h) holds 16 bytes (column half h) of vector b for each chunk of a window
+    __device__ __forceinline__ void load_window(uint4 (&xr)[kXChunks], const int8_t *xrow, bool xok, int colbase,
+                                                int cbase, int nchunks) const {
+#pragma unroll
+        for (int i = 0; i < kXChunks; i++) {
+            const int c = cbase + i;
+            xr[i] = make_uint4(0, 0, 0, 0);
+            // cols % 16 == 0, so a 16-byte piece that starts inside the row ends inside it
+            if (xok && c < nchunks && colbase + 32 * c < cols)
+                xr[i] = __ldg(reinterpret_cast<const uint4 *>(xrow + 32 * c));
+        }
+    }
     template <int ILP>
     __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int,
                                              const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
@@ -572,60 +636,46 @@ struct MmaCons {
         const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
         if (nq <= 0) return;
         const int nchunks = (nq + 7) >> 3;
+        const int b = lane >> 1, h = lane & 1;
+        const bool xok = b < batch;
+        const int colbase = 4 * q0 + 16 * h;
+        const int8_t *xrow = x + (size_t)(xok ? b : 0) * cols + colbase;
+        const uint32_t xdst = xt + (uint32_t)(b >> 3) * 256u + (uint32_t)h * 128u + (uint32_t)(b & 7) * 16u;
+        uint4 xr[kXChunks];
+        load_window(xr, xrow, xok, colbase, 0, nchunks);
         uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
         const uint32_t kend = rows_now[0] * 32 + lane;
-        // x is staged in windows of at most kXChunks chunks (the per-warp x tile)
         for (int c0 = 0; c0 < nchunks; c0 += kXChunks) {
             const int cn = min(kXChunks, nchunks - c0);
-            wait_all(L);  // every earlier MMA has read the previous window
-            for (int p = lane; p < 32 * cn; p += 32) {
-                const int c = p >> 5, b = (p & 31) >> 1, h = p & 1;
-                const int col = 4 * q0 + 32 * (c0 + c) + 16 * h;
-                uint4 v = make_uint4(0, 0, 0, 0);
-                if (b < batch && col < cols) v = __ldg(reinterpret_cast<const uint4 *>(x + (size_t)b * cols + col));
-                const uint32_t dst = xt + (uint32_t)c * 512u + (uint32_t)(b >> 3) * 256u + (uint32_t)h * 128u +
-                                     (uint32_t)(b & 7) * 16u;
-                asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst), "r"(v.x), "r"(v.y), "r"(v.z),
-                             "r"(v.w)
-                             : "memory");
-            }
             for (int c = 0; c < cn; c++) {
                 const int qc = 8 * (c0 + c);
                 uint32_t w[8];
+                if (qc + 8 <= nq) {
 #pragma unroll
-                for (int j = 0; j < 8; j++)
-                    w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
-                const int t = (int)wsel;
-                wsel ^= 1;
-                wait_buf(L, t);
-                const uint32_t tile = t ? wt1 : wt0;
-                const uint32_t dst = tile + (uint32_t)(lane >> 3) * 256u + (uint32_t)(lane & 7) * 16u;
-                asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst), "r"(w[0]), "r"(w[1]), "r"(w[2]),
-                             "r"(w[3])
-                             : "memory");
-                asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst + 128u), "r"(w[4]), "r"(w[5]),
-                             "r"(w[6]), "r"(w[7])
-                             : "memory");
-                fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) {
-                    tcgen05_fence_after();
-                    const uint64_t a = umma_smem_desc(xt + (uint32_t)c * 512u - warp_q * 1024u, 128u, 256u);
-                    const uint64_t bdesc = umma_smem_desc(tile, 128u, 256u);
-                    umma_i8(d_tmem, a, bdesc, umma_idesc_i8(128, 32), any ? 1u : 0u);
-                    umma_commit(&mbar[t]);
+                    for (int j = 0; j < 8; j++) w[j] = q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+                        w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
                 }
-                __syncwarp();
-                any = true;
-                if (t) nc1++;
-                else nc0++;
+                if (c == 0) {
+                    // every MMA of the previous window is done with the x tile and both W tiles
+                    wait_all(L);
+#pragma unroll
+                    for (int i = 0; i < kXChunks; i++)
+                        if (i < cn)
+                            asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 512u),
+                                         "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
+                                         : "memory");
+                    if (c0 + kXChunks < nchunks) load_window(xr, xrow, xok, colbase, c0 + kXChunks, nchunks);
+                }
+                put_tile_and_mma(L, w, c, lane, c == 0);
             }
         }
-        if (nq > 0 && (hi != 0 || lo != P)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+        if (hi != 0 || lo != P) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
     __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
-                                                int W, void *red_smem) {
-        int *red = reinterpret_cast<int *>(red_smem);  // [W][32 rows][16 vectors]
+                                                int W, void *) {
         uint32_t r[32];
         if (any) {
             wait_all(L);
@@ -635,9 +685,12 @@ struct MmaCons {
 #pragma unroll
             for (int j = 0; j < 32; j++) r[j] = 0;
         }
+        // this warp's MMAs are complete, so its own x tile (2 KB) takes its partial sums:
+        // [stripe row j][vector v ^ (j % 16)] (the xor spreads the reads below over the banks)
+        int *red = xbase + warp * (kXBytes / 4);
         if (lane < 16) {
 #pragma unroll
-            for (int j = 0; j < 32; j++) red[(warp * 32 + j) * 16 + lane] = (int)r[j];
+            for (int j = 0; j < 32; j++) red[j * 16 + (lane ^ (j & 15))] = (int)r[j];
         }
         tcgen05_fence_before();
         __syncthreads();
@@ -645,7 +698,7 @@ struct MmaCons {
         for (int t = threadIdx.x; t < 16 * 32; t += blockDim.x) {
             const int v = t >> 5, l = t & 31;
             int sum = 0;
-            for (int w = 0; w < W; w++) sum += red[(w * 32 + l) * 16 + v];
+            for (int w = 0; w < W; w++) sum += xbase[w * (kXBytes / 4) + l * 16 + (v ^ (l & 15))];
             const int row = stripe * 32 + l;
             if (row < m.rows && v < L.batch) {
                 int32_t *dst = J.y + (size_t)v * m.rows + row;
@@ -657,14 +710,14 @@ struct MmaCons {
                 }
             }
         }
-        __syncthreads();
+        __syncthreads();  // the x tiles are written again (tables, x) by the next item
     }
     __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_all(L); }
 };
 
 template <class Cons, int ILP, int DEPTH>
-__global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
-    constexpr int NV = Cons::kNV;
+__global__ void __launch_bounds__(256, Cons::kMinCtas) q8s_kernel(const Q8SLaunch L) {
+    constexpr int NV = Cons::kRedNV;
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = blockDim.x >> 5;
@@ -676,7 +729,10 @@ __global__ void __launch_bounds__(256, 1) q8s_kernel(const Q8SLaunch L) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(red + W * NV * 32);                    // [W][DEPTH]
     uint32_t *toff_s = reinterpret_cast<uint32_t *>(bars + W * DEPTH);                   // [36]
     uint32_t *rows_s = toff_s + 36;                                                      // [W][DEPTH][ILP]
-    uint16_t *tsm = reinterpret_cast<uint16_t *>(rows_s + W * DEPTH * ILP);             // [tbl_stage]
+    // [tbl_stage]: its own region, or the consumer's area when that is free at table rebuilds and large enough
+    uint16_t *tsm = (size_t)L.tbl_stage * 2 <= Cons::tbl_alias_bytes(W)
+                        ? reinterpret_cast<uint16_t *>(extra)
+                        : reinterpret_cast<uint16_t *>(rows_s + W * DEPTH * ILP);
 
     uint32_t *my_bufs = bufs + (size_t)warp * DEPTH * ILP * L.buf_words;
     uint32_t *my_rows = rows_s + warp * DEPTH * ILP;
@@ -827,14 +883,31 @@ __global__ void q8s_scale_atomic_y(const Q8Job *jobs, int njobs, int batch) {
 
 namespace {
 
-size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage, size_t extra) {
-    return 256 * 32 * 4 + extra + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 + (size_t)W * DEPTH * 8 +
-           36 * 4 + (size_t)W * DEPTH * ILP * 4 + (size_t)tbl_stage * 2;
+size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage, size_t extra, size_t tbl_alias) {
+    const size_t tbl = (size_t)tbl_stage * 2 <= tbl_alias ? 0 : (size_t)tbl_stage * 2;
+    return 256 * 32 * 4 + extra + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 +
+           (size_t)W * DEPTH * 8 + 36 * 4 + (size_t)W * DEPTH * ILP * 4 + tbl;
+}
+
+mv_status resident_ctas(const void *kern, size_t smem, int threads, int *out) {
+    int d = 0, smem_sm = 0, reserved = 0;
+    MV_CUDA_TRY(cudaGetDevice(&d), "cudaGetDevice");
+    MV_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, d), "attribute");
+    MV_CUDA_TRY(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, d), "attribute");
+    cudaFuncAttributes fa{};
+    MV_CUDA_TRY(cudaFuncGetAttributes(&fa, kern), "cudaFuncGetAttributes");
+    const int warps = (threads + 31) / 32;
+    const int regs_warp = ((std::max(1, fa.numRegs) * 32 + 255) / 256) * 256;  // allocation unit: 256 per warp
+    int n = std::min(smem_sm / (int)(smem + reserved), (65536 / regs_warp) / warps);
+    n = std::min(n, 64 / warps);
+    *out = std::max(1, n);
+    return MV_OK;
 }
 
 template <class Cons, int ILP, int DEPTH>
 mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t st) {
-    const size_t smem = q8s_smem(Cons::kNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage, Cons::extra_bytes(W));
+    const size_t smem = q8s_smem(Cons::kRedNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage, Cons::extra_bytes(W),
+                                 Cons::tbl_alias_bytes(W));
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch needs %zu B of shared memory (max %d)", smem,
                     max_smem_optin());
@@ -843,7 +916,14 @@ mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t 
     mv_status rc = prepare_kernel((const void *)kern, smem, 32 * W, &bps);
     if (rc) return rc;
     if (ctas_per_sm > 0) bps = std::min(bps, ctas_per_sm);
-    if (Cons::kTmemCols) bps = std::max(1, std::min<int>(bps, 512 / MmaCons::tmem_cols(W)));
+    if (Cons::kTmemCols) {
+        // resident CTAs of a tensor-memory kernel, from its resources directly: shared memory, registers,
+        // threads and TMEM columns (512 per SM)
+        rc = resident_ctas((const void *)kern, smem, 32 * W, &bps);
+        if (rc) return rc;
+        if (ctas_per_sm > 0) bps = std::min(bps, ctas_per_sm);
+        bps = std::max(1, std::min<int>(bps, 512 / MmaCons::tmem_cols(W)));
+    }
     const long long grid = std::max(1LL, std::min<long long>(L.nitems, (long long)bps * sm_count()));
     kern<<<(unsigned)grid, 32 * W, smem, st>>>(L);
     MV_CUDA_TRY(cudaGetLastError(), "q8 stack kernel launch");
