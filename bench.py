@@ -565,14 +565,16 @@ def run_profile_stack(args):
     """Small fixed stack case for ncu: gate + two plain steps."""
     import torch
     from matvans_b200 import ops
-    layers, B, engine = (int(v) for v in args.profile_stack.split(","))
+    vals = [int(v) for v in args.profile_stack.split(",")]
+    layers, B, engine = vals[:3]
+    warps = vals[3] if len(vals) > 3 else 4
     dev = torch.device("cuda", 0)
     mats = build_stack(torch, ops, dev, layers)
     Ms = [m["M"] for m in mats]
     g = torch.Generator(device=dev)
     g.manual_seed(99)
     xs = [torch.randint(-127, 128, (B, M.cols), dtype=torch.int8, device=dev, generator=g) for M in Ms]
-    S = ops.Q8Stack(Ms, batch=B, tuning=(4, 1, 1, 0, 0, engine), xs=xs, device=dev)
+    S = ops.Q8Stack(Ms, batch=B, tuning=(warps, 1, 1, 0, 0, engine), xs=xs, device=dev)
     S.run()
     for m, x, y in zip(mats, xs, S.ys):
         if not torch.equal(y, ops.dense_matvec(m["Wd"], x)):
@@ -593,8 +595,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stack", action="store_true", help="skip the 224-matrix batched stack section")
     ap.add_argument("--profile-stack", default="",
-                    help="LAYERS,B,ENGINE: build a stack of LAYERS x 7 matrices and run two steps at B vectors "
-                         "with the given engine (the case ncu captures)")
+                    help="LAYERS,B,ENGINE[,WARPS]: build a stack of LAYERS x 7 matrices and run two steps at B "
+                         "vectors with the given engine and warps per CTA (the case ncu captures)")
     ap.add_argument("--tuning", default="", help="fixed stack launch parameters warps,ilp,depth,ctas_per_sm "
                                                   "(default: autotuned)")
     ap.add_argument("--profile", action="store_true",

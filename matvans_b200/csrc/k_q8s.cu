@@ -513,18 +513,19 @@ __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const 
 
 // y = W x for 8..16 int8 vectors on the tensor cores.  Every 8 decoded quads
 // the 32 lanes of a warp (= the 32 rows of the stripe) hold a 32 x 32 int8
-// tile of W; it is written to shared memory in the canonical K-major layout
-// (8-row x 16-byte core matrices, LBO 128 B, SBO 256 B) and one lane issues
-// tcgen05.mma.kind::i8 with M = 128 (A = the x tile; only the rows of this
-// warp's TMEM lane quarter hold the real vectors, the others are ignored),
-// N = 32 (B = the W tile), K = 32, accumulating exactly in int32 in the warp's
-// own 32 TMEM columns.  W tiles are double-buffered; a tcgen05.commit to an
-// mbarrier tells when a tile may be overwritten.  x moves through a 4-chunk
-// window (4 x 32 columns x 16 vectors); the next window is loaded into
-// registers while the current one is in use.  Shared memory per warp is kept
-// small so that 12-16 warps fit on an SM: the x tiles double as the
-// cross-warp reduction area and as the staging area of the decode tables.
-// ILP 1 only.
+// tile of W, one row per lane: each lane writes its row straight from
+// registers into its own TMEM lane (tcgen05.st), and one lane issues
+// tcgen05.mma.kind::i8 with A = that tile in TMEM (M = 128: the warp's lane
+// quarter holds its 32 rows, the other lanes are never written and their
+// results never read), B = the x tile in shared memory (N = 16 vectors,
+// K-major core matrices of 8 rows x 16 bytes, LBO 128 B, SBO 256 B), K = 32,
+// accumulating exactly in int32 in the warp's own 16 TMEM columns.  Each warp
+// owns 32 TMEM columns: D [0,16), two A tiles [16,24) and [24,32); a
+// tcgen05.commit to an mbarrier tells when an A tile may be overwritten.
+// x moves through a 4-chunk window (4 x 32 columns x 16 vectors, 2 KB per
+// warp); the next window is loaded into registers while the current one is in
+// use.  The x tiles double as the cross-warp reduction area and as the
+// staging area of the decode tables.  ILP 1 only.
 struct MmaCons {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;      // reduction area: the x tiles
@@ -533,19 +534,16 @@ struct MmaCons {
     static constexpr int kXChunks = 4;    // x tile: 4 chunks of 32 columns x 16 vectors (512 B each)
     static constexpr int kXBytes = kXChunks * 512;
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
-        // x tile 2 KB + W tiles 2 x 1 KB per warp, 2 mbarriers per warp, TMEM address slot; at least the
-        // span an A operand reads (16 row groups of 256 B from the last chunk of the last x tile), so that
-        // the ignored rows never reach past this region
-        return std::max<size_t>((size_t)W * (kXBytes + 2048) + (size_t)W * 16 + 128,
-                                (size_t)(W - 1) * kXBytes + (kXChunks - 1) * 512 + 16 * 256 + 128);
+        // x tile 2 KB per warp, 2 mbarriers per warp, TMEM address slot
+        return (size_t)W * kXBytes + (size_t)W * 16 + 128;
     }
     // the decode tables are staged in the x tiles when they fit
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)W * kXBytes; }
     static __host__ __device__ constexpr uint32_t tmem_cols(int W) {
         return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : W <= 8 ? 256 : 512;
     }
-    uint32_t xt, wt0, d_tmem, ld_addr, nc0, nc1, wsel;
-    uint64_t a_desc0, b_desc0;
+    uint32_t xt, d_tmem, a_tmem0, st_addr0, ld_addr, nc0, nc1, wsel;
+    uint64_t b_desc0;
     uint64_t *mbar;
     int *xbase;
     const int8_t *x;
@@ -557,21 +555,21 @@ struct MmaCons {
         const uint32_t base = smem_u32(extra);
         xbase = reinterpret_cast<int *>(extra);
         xt = base + (uint32_t)warp * (uint32_t)kXBytes;
-        wt0 = base + (uint32_t)W * (uint32_t)kXBytes + (uint32_t)warp * 2048u;
-        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * (kXBytes + 2048)) + 2 * warp;
+        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * kXBytes) + 2 * warp;
         if (lane == 0) {
             mbar_init(&mbar[0], 1);
             mbar_init(&mbar[1], 1);
         }
         fence_mbar_init();
         __syncwarp();
-        const uint32_t warp_q = (uint32_t)(warp & 3);
+        // TMEM addresses: lane in bits [16,32), column in [0,16); a warp may touch only the 32 lanes of its
+        // quarter (warp % 4) with tcgen05.ld/st, while an MMA with M = 128 addresses lanes from 0
+        const uint32_t quarter = ((uint32_t)(warp & 3) * 32u) << 16;
         d_tmem = tmem_base + 32u * (uint32_t)warp;
-        ld_addr = tmem_base + ((32u * warp_q) << 16) + 32u * (uint32_t)warp;
-        // A starts 4 * warp_q row groups (1 KB each) before the x tile, so vector b lands in TMEM lane
-        // 32 * warp_q + b; the x tiles follow the 32 KB decode table, so the start stays in shared memory
-        a_desc0 = umma_smem_desc(xt - warp_q * 1024u, 128u, 256u);
-        b_desc0 = umma_smem_desc(wt0, 128u, 256u);
+        a_tmem0 = d_tmem + 16u;
+        st_addr0 = a_tmem0 + quarter;
+        ld_addr = d_tmem + quarter;
+        b_desc0 = umma_smem_desc(xt, 128u, 256u);
         nc0 = nc1 = wsel = 0;
     }
     __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
@@ -580,7 +578,7 @@ struct MmaCons {
         batch = L.batch;
         any = false;
     }
-    // wait until the MMA that last read W-tile buffer t (and all earlier ones) completed
+    // wait until the MMA that last read A tile t (and all earlier ones) completed
     __device__ __forceinline__ bool wait_buf(const Q8SLaunch &L, int t) {
         const uint32_t n = t ? nc1 : nc0;
         if (n == 0) return true;
@@ -596,19 +594,15 @@ struct MmaCons {
         const int t = (int)wsel;
         if (!waited) wait_buf(L, t);
         wsel ^= 1;
-        const uint32_t dst = wt0 + (uint32_t)t * 1024u + (uint32_t)(lane >> 3) * 256u + (uint32_t)(lane & 7) * 16u;
-        asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst), "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3])
-                     : "memory");
-        asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(dst + 128u), "r"(w[4]), "r"(w[5]), "r"(w[6]),
-                     "r"(w[7])
-                     : "memory");
-        fence_proxy_async_smem();
+        tcgen05_fence_after();
+        tmem_st_32x32b_x8(st_addr0 + 8u * (uint32_t)t, w);
+        tcgen05_fence_before();
         __syncwarp();
         if (lane == 0) {
             tcgen05_fence_after();
-            // descriptor start addresses are in 16-byte units: chunk c of the x tile is 512 B in, tile t 1 KB
-            umma_i8(d_tmem, a_desc0 + (uint64_t)(c * 32), b_desc0 + (uint64_t)(t * 64), umma_idesc_i8(128, 32),
-                    any ? 1u : 0u);
+            // B descriptor start addresses are in 16-byte units: chunk c of the x tile is 512 B in
+            umma_i8_ts(d_tmem, a_tmem0 + 8u * (uint32_t)t, b_desc0 + (uint64_t)(c * 32), umma_idesc_i8(128, 16),
+                       any ? 1u : 0u);
             umma_commit(&mbar[t]);
         }
         any = true;
@@ -659,7 +653,7 @@ struct MmaCons {
                         w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
                 }
                 if (c == 0) {
-                    // every MMA of the previous window is done with the x tile and both W tiles
+                    // every MMA of the previous window is done with the x tile and both A tiles
                     wait_all(L);
 #pragma unroll
                     for (int i = 0; i < kXChunks; i++)
@@ -667,6 +661,7 @@ struct MmaCons {
                             asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 512u),
                                          "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
                                          : "memory");
+                    fence_proxy_async_smem();  // the x tile is read by the tensor core (async proxy)
                     if (c0 + kXChunks < nchunks) load_window(xr, xrow, xok, colbase, c0 + kXChunks, nchunks);
                 }
                 put_tile_and_mma(L, w, c, lane, c == 0);
@@ -676,29 +671,26 @@ struct MmaCons {
     }
     __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
                                                 int W, void *) {
-        uint32_t r[32];
+        uint32_t r[16];
         if (any) {
             wait_all(L);
             tcgen05_fence_after();
-            tmem_ld_32x32b_x32(ld_addr, r);
+            tmem_ld_32x32b_x16(ld_addr, r);  // lane = stripe row, r[v] = vector v
         } else {
 #pragma unroll
-            for (int j = 0; j < 32; j++) r[j] = 0;
+            for (int v = 0; v < 16; v++) r[v] = 0;
         }
-        // this warp's MMAs are complete, so its own x tile (2 KB) takes its partial sums:
-        // [stripe row j][vector v ^ (j % 16)] (the xor spreads the reads below over the banks)
+        // this warp's MMAs are complete, so its own x tile (2 KB) takes its partial sums: [vector][stripe row]
         int *red = xbase + warp * (kXBytes / 4);
-        if (lane < 16) {
 #pragma unroll
-            for (int j = 0; j < 32; j++) red[j * 16 + (lane ^ (j & 15))] = (int)r[j];
-        }
+        for (int v = 0; v < 16; v++) red[v * 32 + lane] = (int)r[v];
         tcgen05_fence_before();
         __syncthreads();
         const mv_q8_view &m = J.m;
         for (int t = threadIdx.x; t < 16 * 32; t += blockDim.x) {
             const int v = t >> 5, l = t & 31;
             int sum = 0;
-            for (int w = 0; w < W; w++) sum += xbase[w * (kXBytes / 4) + l * 16 + (v ^ (l & 15))];
+            for (int w = 0; w < W; w++) sum += xbase[w * (kXBytes / 4) + t];
             const int row = stripe * 32 + l;
             if (row < m.rows && v < L.batch) {
                 int32_t *dst = J.y + (size_t)v * m.rows + row;
