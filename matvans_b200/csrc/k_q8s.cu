@@ -511,38 +511,41 @@ __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const 
     decode_step<BwdCons<NV>, ILP>(L, m, seg0, W, rows_now, sb, lut_l, lane, *this);
 }
 
-// y = W x for 8..16 int8 vectors on the tensor cores.  Every 8 decoded quads
-// the 32 lanes of a warp (= the 32 rows of the stripe) hold a 32 x 32 int8
+// y = W x for 8..16 int8 vectors on the tensor cores.  Every 16 decoded quads
+// the 32 lanes of a warp (= the 32 rows of the stripe) hold a 32 x 64 int8
 // tile of W, one row per lane: each lane writes its row straight from
-// registers into its own TMEM lane (tcgen05.st), and one lane issues
-// tcgen05.mma.kind::i8 with A = that tile in TMEM (M = 128: the warp's lane
-// quarter holds its 32 rows, the other lanes are never written and their
-// results never read), B = the x tile in shared memory (N = 16 vectors,
-// K-major core matrices of 8 rows x 16 bytes, LBO 128 B, SBO 256 B), K = 32,
-// accumulating exactly in int32 in the warp's own 16 TMEM columns.  Each warp
-// owns 32 TMEM columns: D [0,16), two A tiles [16,24) and [24,32); a
-// tcgen05.commit to an mbarrier tells when an A tile may be overwritten.
-// x moves through a 4-chunk window (4 x 32 columns x 16 vectors, 2 KB per
-// warp); the next window is loaded into registers while the current one is in
-// use.  The x tiles double as the cross-warp reduction area and as the
-// staging area of the decode tables.  ILP 1 only.
+// registers into its own TMEM lane (tcgen05.st, 8 quads at a time), and one
+// lane issues two tcgen05.mma.kind::i8 (K = 32 each) with A = that tile in
+// TMEM (M = 128: the warp's lane quarter holds its 32 rows, the other lanes
+// are never written and their results never read), B = the x tile in shared
+// memory (N = 16 vectors, K-major core matrices of 8 rows x 16 bytes, LBO
+// 128 B, SBO 256 B), accumulating exactly in int32 in the warp's own 16 TMEM
+// columns.  Each warp owns 32 TMEM columns: D [0,16) and the A tile [16,32).
+// One tcgen05.commit per 16 quads arrives on the warp's mbarrier; the A tile
+// is rewritten only after the previous pair of MMAs completed (issued a whole
+// 16-quad decode earlier, so the wait is normally already over).  x moves
+// through a 128-column window (4 x 32 columns x 16 vectors, 2 KB per warp);
+// the next window is loaded into registers while the current one is in use.
+// The x tiles double as the cross-warp reduction area and as the staging area
+// of the decode tables.  ILP 1 only.
 struct MmaCons {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;      // reduction area: the x tiles
     static constexpr int kMinCtas = 2;    // 2 x 8 warps per SM: at most 128 registers per thread
     static constexpr int kTmemCols = 1;   // > 0: the kernel allocates TMEM
-    static constexpr int kXChunks = 4;    // x tile: 4 chunks of 32 columns x 16 vectors (512 B each)
+    static constexpr int kXChunks = 4;    // x tile: 4 pieces of 32 columns x 16 vectors (512 B each)
     static constexpr int kXBytes = kXChunks * 512;
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
-        // x tile 2 KB per warp, 2 mbarriers per warp, TMEM address slot
-        return (size_t)W * kXBytes + (size_t)W * 16 + 128;
+        // x tile 2 KB per warp, one mbarrier per warp, TMEM address slot (the last 128 bytes); a multiple
+        // of 128 bytes, so the stream buffers that follow stay 16-byte aligned for the bulk copies
+        return (((size_t)W * kXBytes + (size_t)W * 8 + 128) + 127) / 128 * 128;
     }
     // the decode tables are staged in the x tiles when they fit
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)W * kXBytes; }
     static __host__ __device__ constexpr uint32_t tmem_cols(int W) {
         return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : W <= 8 ? 256 : 512;
     }
-    uint32_t xt, d_tmem, a_tmem0, st_addr0, ld_addr, nc0, nc1, wsel;
+    uint32_t xt, d_tmem, st_addr, ld_addr, ncommit;
     uint64_t b_desc0;
     uint64_t *mbar;
     int *xbase;
@@ -550,27 +553,26 @@ struct MmaCons {
     int cols, batch;
     bool any;
 
-    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int warp,
+    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int,
                                          int lane, int W) {
+        // the warp index through a shuffle from lane 0 is known warp-uniform to the compiler, so the MMA
+        // operands derived from it stay in uniform registers
+        const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
         const uint32_t base = smem_u32(extra);
         xbase = reinterpret_cast<int *>(extra);
         xt = base + (uint32_t)warp * (uint32_t)kXBytes;
-        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * kXBytes) + 2 * warp;
-        if (lane == 0) {
-            mbar_init(&mbar[0], 1);
-            mbar_init(&mbar[1], 1);
-        }
+        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * kXBytes) + warp;
+        if (lane == 0) mbar_init(mbar, 1);
         fence_mbar_init();
         __syncwarp();
         // TMEM addresses: lane in bits [16,32), column in [0,16); a warp may touch only the 32 lanes of its
         // quarter (warp % 4) with tcgen05.ld/st, while an MMA with M = 128 addresses lanes from 0
         const uint32_t quarter = ((uint32_t)(warp & 3) * 32u) << 16;
         d_tmem = tmem_base + 32u * (uint32_t)warp;
-        a_tmem0 = d_tmem + 16u;
-        st_addr0 = a_tmem0 + quarter;
+        st_addr = d_tmem + 16u + quarter;
         ld_addr = d_tmem + quarter;
         b_desc0 = umma_smem_desc(xt, 128u, 256u);
-        nc0 = nc1 = wsel = 0;
+        ncommit = 0;
     }
     __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
         x = J.x;
@@ -578,46 +580,35 @@ struct MmaCons {
         batch = L.batch;
         any = false;
     }
-    // wait until the MMA that last read A tile t (and all earlier ones) completed
-    __device__ __forceinline__ bool wait_buf(const Q8SLaunch &L, int t) {
-        const uint32_t n = t ? nc1 : nc0;
-        if (n == 0) return true;
-        return mbar_wait_bounded(&mbar[t], (n - 1) & 1, L.status, L.spin_limit);
+    // wait until every MMA issued so far completed (the latest commit covers all earlier MMAs)
+    __device__ __forceinline__ bool wait_mma(const Q8SLaunch &L) {
+        if (ncommit == 0) return true;
+        return mbar_wait_bounded(mbar, (ncommit - 1) & 1, L.status, L.spin_limit);
     }
-    __device__ __forceinline__ bool wait_all(const Q8SLaunch &L) {
-        // the most recent commit covers every earlier MMA of this thread
-        const int last = wsel ^ 1;
-        return wait_buf(L, last) && wait_buf(L, last ^ 1);
-    }
-    __device__ __forceinline__ void put_tile_and_mma(const Q8SLaunch &L, const uint32_t (&w)[8], int c, int lane,
-                                                     bool waited) {
-        const int t = (int)wsel;
-        if (!waited) wait_buf(L, t);
-        wsel ^= 1;
-        tcgen05_fence_after();
-        tmem_st_32x32b_x8(st_addr0 + 8u * (uint32_t)t, w);
+    __device__ __forceinline__ void issue(int piece, bool two) {
         tcgen05_fence_before();
         __syncwarp();
-        if (lane == 0) {
+        if (elect_one()) {
             tcgen05_fence_after();
-            // B descriptor start addresses are in 16-byte units: chunk c of the x tile is 512 B in
-            umma_i8_ts(d_tmem, a_tmem0 + 8u * (uint32_t)t, b_desc0 + (uint64_t)(c * 32), umma_idesc_i8(128, 16),
-                       any ? 1u : 0u);
-            umma_commit(&mbar[t]);
+            // B descriptor start addresses are in 16-byte units: x piece p is 512 B into the x tile
+            const uint32_t idesc = umma_idesc_i8(128, 16);
+            umma_i8_ts(d_tmem, d_tmem + 16u, b_desc0 + (uint64_t)(piece * 32), idesc, any ? 1u : 0u);
+            if (two) umma_i8_ts(d_tmem, d_tmem + 24u, b_desc0 + (uint64_t)(piece * 32 + 32), idesc, 1u);
+            umma_commit(mbar);
         }
+        __syncwarp();
         any = true;
-        if (t) nc1++;
-        else nc0++;
+        ncommit++;
     }
-    // lane (b, h) holds 16 bytes (column half h) of vector b for each chunk of a window
+    // lane (b, h) holds 16 bytes (column half h) of vector b for each 32-column piece of a window
     __device__ __forceinline__ void load_window(uint4 (&xr)[kXChunks], const int8_t *xrow, bool xok, int colbase,
-                                                int cbase, int nchunks) const {
+                                                int pbase, int npieces) const {
 #pragma unroll
         for (int i = 0; i < kXChunks; i++) {
-            const int c = cbase + i;
+            const int c = pbase + i;
             xr[i] = make_uint4(0, 0, 0, 0);
             // cols % 16 == 0, so a 16-byte piece that starts inside the row ends inside it
-            if (xok && c < nchunks && colbase + 32 * c < cols)
+            if (xok && c < npieces && colbase + 32 * c < cols)
                 xr[i] = __ldg(reinterpret_cast<const uint4 *>(xrow + 32 * c));
         }
     }
@@ -629,43 +620,59 @@ struct MmaCons {
         const int q0 = seg0 * m.seg_quads;
         const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
         if (nq <= 0) return;
-        const int nchunks = (nq + 7) >> 3;
+        const int npieces = (nq + 7) >> 3;  // 32-column pieces (8 quads each)
         const int b = lane >> 1, h = lane & 1;
         const bool xok = b < batch;
         const int colbase = 4 * q0 + 16 * h;
         const int8_t *xrow = x + (size_t)(xok ? b : 0) * cols + colbase;
         const uint32_t xdst = xt + (uint32_t)(b >> 3) * 256u + (uint32_t)h * 128u + (uint32_t)(b & 7) * 16u;
         uint4 xr[kXChunks];
-        load_window(xr, xrow, xok, colbase, 0, nchunks);
+        load_window(xr, xrow, xok, colbase, 0, npieces);
         uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
         const uint32_t kend = rows_now[0] * 32 + lane;
-        for (int c0 = 0; c0 < nchunks; c0 += kXChunks) {
-            const int cn = min(kXChunks, nchunks - c0);
-            for (int c = 0; c < cn; c++) {
-                const int qc = 8 * (c0 + c);
-                uint32_t w[8];
-                if (qc + 8 <= nq) {
+        // pieces in pairs: piece p = 2 * pair (+1); a window holds 2 pairs
+        for (int p = 0; p < npieces; p += 2) {
+            uint32_t w[8];
+            const int qc = 8 * p;
+            if (qc + 8 <= nq) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) w[j] = q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
+            }
+            // the previous pair of MMAs is done with the A tile (and, at a window start, with the x tile)
+            wait_mma(L);
+            const int pw = p & (kXChunks - 1);  // piece within the window
+            if (pw == 0) {
+                const int cn = min(kXChunks, npieces - p);
+#pragma unroll
+                for (int i = 0; i < kXChunks; i++)
+                    if (i < cn)
+                        asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 512u),
+                                     "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
+                                     : "memory");
+                fence_proxy_async_smem();  // the x tile is read by the tensor core (async proxy)
+                if (p + kXChunks < npieces) load_window(xr, xrow, xok, colbase, p + kXChunks, npieces);
+            }
+            tcgen05_fence_after();
+            tmem_st_32x32b_x8_nowait(st_addr, w);
+            const bool two = p + 1 < npieces;
+            if (two) {
+                const int qc2 = qc + 8;
+                if (qc2 + 8 <= nq) {
 #pragma unroll
                     for (int j = 0; j < 8; j++) w[j] = q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 8; j++)
-                        w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
+                        w[j] = (qc2 + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
                 }
-                if (c == 0) {
-                    // every MMA of the previous window is done with the x tile and both A tiles
-                    wait_all(L);
-#pragma unroll
-                    for (int i = 0; i < kXChunks; i++)
-                        if (i < cn)
-                            asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 512u),
-                                         "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
-                                         : "memory");
-                    fence_proxy_async_smem();  // the x tile is read by the tensor core (async proxy)
-                    if (c0 + kXChunks < nchunks) load_window(xr, xrow, xok, colbase, c0 + kXChunks, nchunks);
-                }
-                put_tile_and_mma(L, w, c, lane, c == 0);
+                tmem_st_32x32b_x8_nowait(st_addr + 8u, w);
             }
+            tmem_wait_st();
+            issue(pw, two);
         }
         if (hi != 0 || lo != P) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
@@ -673,7 +680,7 @@ struct MmaCons {
                                                 int W, void *) {
         uint32_t r[16];
         if (any) {
-            wait_all(L);
+            wait_mma(L);
             tcgen05_fence_after();
             tmem_ld_32x32b_x16(ld_addr, r);  // lane = stripe row, r[v] = vector v
         } else {
@@ -704,7 +711,7 @@ struct MmaCons {
         }
         __syncthreads();  // the x tiles are written again (tables, x) by the next item
     }
-    __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_all(L); }
+    __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_mma(L); }
 };
 
 template <class Cons, int ILP, int DEPTH>
@@ -898,6 +905,9 @@ mv_status resident_ctas(const void *kern, size_t smem, int threads, int *out) {
 
 template <class Cons, int ILP, int DEPTH>
 mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t st) {
+    if (Cons::extra_bytes(W) % 16)  // the stream buffers behind the consumer region take bulk copies
+        return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch: consumer region of %zu B breaks 16-byte alignment",
+                    Cons::extra_bytes(W));
     const size_t smem = q8s_smem(Cons::kRedNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage, Cons::extra_bytes(W),
                                  Cons::tbl_alias_bytes(W));
     if (smem > (size_t)max_smem_optin())

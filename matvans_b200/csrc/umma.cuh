@@ -73,6 +73,27 @@ __device__ __forceinline__ void tmem_ld_32x32b_x16(uint32_t taddr, uint32_t (&r)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Whole warp: lane i writes r[0..7] to 8 consecutive 32-bit columns of TMEM
+// lane (taddr.lane + i) without waiting for completion (see tmem_wait_st).
+__device__ __forceinline__ void tmem_st_32x32b_x8_nowait(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Whole warp: true in exactly one lane.
+__device__ __forceinline__ bool elect_one() {
+    uint32_t p = 0;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "elect.sync _|P, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, P;\n\t}"
+        : "=r"(p));
+    return p != 0;
+}
+
 // Arrive once on `bar` when every tcgen05 operation issued so far by this
 // thread has completed.
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
