@@ -31,6 +31,8 @@
 #include <algorithm>
 #include <cstdio>
 
+#include <cuda_bf16.h>
+
 #include "mv_device.cuh"
 #include "umma.cuh"
 
@@ -714,6 +716,348 @@ struct MmaCons {
     __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_mma(L); }
 };
 
+// four int8 weights (packed) -> four bf16 (exact: |w| <= 127 needs 7 significand bits), as two bf16x2
+// words in column order: lo = (w0, w1), hi = (w2, w3)
+__device__ __forceinline__ void i8x4_to_bf16x4(uint32_t wq, uint32_t &lo, uint32_t &hi) {
+    float f[4];
+    i8x4_to_f32(wq, f);
+    lo = __byte_perm(__float_as_uint(f[0]), __float_as_uint(f[1]), 0x7632);
+    hi = __byte_perm(__float_as_uint(f[2]), __float_as_uint(f[3]), 0x7632);
+}
+
+// Decode one 8-quad piece of the lane's row (zeros past nq).
+__device__ __forceinline__ void decode_piece(int qc, int nq, uint32_t &lo, uint32_t &hi, uint32_t &k, uint32_t kend,
+                                             const uint32_t *sb, const uint32_t *lut_l, uint32_t stride, uint32_t &P,
+                                             uint32_t (&w)[8]) {
+    if (qc + 8 <= nq) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) w[j] = q8_step(lo, hi, k, kend, sb, lut_l, stride, P);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, stride, P) : 0u;
+    }
+}
+
+// Float forward on the tensor cores: Y = diag(s) W X for up to 16 bf16 vectors,
+// fp32 accumulation (kind::f16 MMAs, bf16 A and B: the int8 weights and the bf16
+// inputs are exact in bf16, every product is exact in fp32).  Per 8 decoded
+// quads each lane converts its 32 weights to bf16 and stores them into its
+// TMEM lane (A, 16 columns); one lane issues two MMAs (K = 16 each) against the
+// x tile (B: 16 vectors x 32 columns of bf16, K-major core matrices, 1 KB) into
+// the warp's 16 fp32 D columns.  x moves through a 2-piece window (2 KB per
+// warp) loaded into registers ahead of use.  The x tiles hold the cross-warp
+// reduction (fixed order) at the end of a stripe and stage the decode tables.
+struct FwdMma {
+    static constexpr int kNV = 16;
+    static constexpr int kRedNV = 0;
+    static constexpr int kMinCtas = 2;
+    static constexpr int kTmemCols = 1;
+    static constexpr int kXPieces = 2;
+    static constexpr int kXBytes = kXPieces * 1024;
+    static __host__ __device__ constexpr size_t extra_bytes(int W) {
+        return (((size_t)W * kXBytes + (size_t)W * 8 + 128) + 127) / 128 * 128;
+    }
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)W * kXBytes; }
+    uint32_t xt, d_tmem, st_addr, ld_addr, ncommit;
+    uint64_t b_desc0;
+    uint64_t *mbar;
+    float *xbase;
+    const uint16_t *x;
+    int cols, batch;
+    bool any;
+
+    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int, int lane,
+                                         int W) {
+        const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+        const uint32_t base = smem_u32(extra);
+        xbase = reinterpret_cast<float *>(extra);
+        xt = base + (uint32_t)warp * (uint32_t)kXBytes;
+        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * kXBytes) + warp;
+        if (lane == 0) mbar_init(mbar, 1);
+        fence_mbar_init();
+        __syncwarp();
+        const uint32_t quarter = ((uint32_t)(warp & 3) * 32u) << 16;
+        d_tmem = tmem_base + 32u * (uint32_t)warp;
+        st_addr = d_tmem + 16u + quarter;
+        ld_addr = d_tmem + quarter;
+        b_desc0 = umma_smem_desc(xt, 128u, 256u);
+        ncommit = 0;
+    }
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
+        x = reinterpret_cast<const uint16_t *>(J.x);
+        cols = J.m.cols;
+        batch = L.batch;
+        any = false;
+    }
+    __device__ __forceinline__ bool wait_mma(const Q8SLaunch &L) {
+        if (ncommit == 0) return true;
+        return mbar_wait_bounded(mbar, (ncommit - 1) & 1, L.status, L.spin_limit);
+    }
+    // lane (b, hh) moves vector b's 8-column chunks 2*hh and 2*hh+1 of each 32-column piece of a window
+    __device__ __forceinline__ void load_window(uint4 (&xr)[2 * kXPieces], const uint16_t *xrow, bool xok,
+                                                int colbase, int pbase, int npieces) const {
+#pragma unroll
+        for (int i = 0; i < kXPieces; i++) {
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const int p = pbase + i;
+                const int off = 32 * p + 8 * j;  // columns from xrow
+                xr[2 * i + j] = make_uint4(0, 0, 0, 0);
+                // cols % 16 == 0: an 8-column chunk that starts inside the row ends inside it
+                if (xok && p < npieces && colbase + off < cols)
+                    xr[2 * i + j] = __ldg(reinterpret_cast<const uint4 *>(xrow + off));
+            }
+        }
+    }
+    template <int ILP>
+    __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int,
+                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
+                                             int lane) {
+        const int qtot = (m.cols + 3) >> 2;
+        const int q0 = seg0 * m.seg_quads;
+        const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
+        if (nq <= 0) return;
+        const int npieces = (nq + 7) >> 3;
+        const int b = lane >> 1, hh = lane & 1;
+        const bool xok = b < batch;
+        const int colbase = 4 * q0 + 16 * hh;
+        const uint16_t *xrow = x + (size_t)(xok ? b : 0) * cols + colbase;
+        // chunk c8 = 2 hh + j of a piece: K step c8 >> 1 (512 B), K half c8 & 1 (128 B)
+        const uint32_t xdst = xt + (uint32_t)hh * 512u + (uint32_t)(b >> 3) * 256u + (uint32_t)(b & 7) * 16u;
+        uint4 xr[2 * kXPieces];
+        load_window(xr, xrow, xok, colbase, 0, npieces);
+        uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
+        const uint32_t kend = rows_now[0] * 32 + lane;
+        for (int p = 0; p < npieces; p++) {
+            uint32_t w[8];
+            decode_piece(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, P, w);
+            uint32_t a[16];
+#pragma unroll
+            for (int j = 0; j < 8; j++) i8x4_to_bf16x4(w[j], a[2 * j], a[2 * j + 1]);
+            wait_mma(L);  // the previous MMAs are done with the A columns (and the x tile)
+            const int pw = p & (kXPieces - 1);
+            if (pw == 0) {
+                const int cn = min(kXPieces, npieces - p);
+#pragma unroll
+                for (int i = 0; i < kXPieces; i++)
+                    if (i < cn) {
+#pragma unroll
+                        for (int j = 0; j < 2; j++) {
+                            const uint4 v = xr[2 * i + j];
+                            asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(
+                                             xdst + (uint32_t)i * 1024u + (uint32_t)j * 128u),
+                                         "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+                                         : "memory");
+                        }
+                    }
+                fence_proxy_async_smem();
+                if (p + kXPieces < npieces) load_window(xr, xrow, xok, colbase, p + kXPieces, npieces);
+            }
+            tcgen05_fence_after();
+            tmem_st_32x32b_x16_nowait(st_addr, a);
+            tmem_wait_st();
+            tcgen05_fence_before();
+            __syncwarp();
+            if (elect_one()) {
+                tcgen05_fence_after();
+                const uint32_t idesc = umma_idesc_bf16(128, 16, 0, 0);
+                const uint64_t bd = b_desc0 + (uint64_t)(pw * 64);  // 1 KB per piece, in 16-byte units
+                umma_f16_ts(d_tmem, d_tmem + 16u, bd, idesc, any ? 1u : 0u);
+                umma_f16_ts(d_tmem, d_tmem + 24u, bd + 32u, idesc, 1u);
+                umma_commit(mbar);
+            }
+            __syncwarp();
+            any = true;
+            ncommit++;
+        }
+        if (hi != 0 || lo != P) atomicOr(L.status, MV_DEV_FINAL_STATE);
+    }
+    __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
+                                                int W, void *) {
+        uint32_t r[16];
+        if (any) {
+            wait_mma(L);
+            tcgen05_fence_after();
+            tmem_ld_32x32b_x16(ld_addr, r);  // lane = stripe row, r[v] = vector v (fp32 bits)
+        } else {
+#pragma unroll
+            for (int v = 0; v < 16; v++) r[v] = 0;
+        }
+        float *red = xbase + warp * (kXBytes / 4);
+#pragma unroll
+        for (int v = 0; v < 16; v++) red[v * 32 + lane] = __uint_as_float(r[v]);
+        tcgen05_fence_before();
+        __syncthreads();
+        const mv_q8_view &m = J.m;
+        for (int t = threadIdx.x; t < 16 * 32; t += blockDim.x) {
+            const int v = t >> 5, l = t & 31;
+            float sum = 0.f;
+            for (int w = 0; w < W; w++) sum += xbase[w * (kXBytes / 4) + t];  // fixed order: deterministic
+            const int row = stripe * 32 + l;
+            if (row < m.rows && v < L.batch) {
+                float *dst = J.ys + (size_t)v * m.rows + row;
+                const float val = sum * J.scales[row];
+                if (J.atomic) atomicAdd(dst, val);
+                else *dst = val;
+            }
+        }
+        __syncthreads();
+    }
+    __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_mma(L); }
+};
+
+// Float backward on the tensor cores: dX = W^T (s . dY) for up to 32 bf16
+// vectors.  Per stripe the CTA builds G = s . dY for its 32 rows as a pair of
+// bf16 tiles, hi = bf16(g) and lo = bf16(g - hi), so that hi + lo carries g to
+// ~16 significant bits (K-major, 32 vectors x 32 rows, 4 KB, shared by the
+// warps).  Per 8 decoded quads each lane converts its 32 weights to bf16 and
+// writes them into the warp's W tile in shared memory (MN-major: the tile is
+// B = W^T's transpose as stored, N = 32 columns, K = 32 rows); one lane issues
+// four MMAs (K = 16 rows each, hi and lo) with A = G (M = 128, the start moved
+// back by the warp's lane quarter so that vector v lands in TMEM lane
+// 32 (warp % 4) + v; the other rows are ignored) into the warp's 32 fp32 D
+// columns.  The D tile of a piece is read back while the next piece decodes
+// and added to dX (fp32, zeroed by the launcher) with 16-byte vector reductions.
+struct BwdMma {
+    static constexpr int kNV = 32;
+    static constexpr int kRedNV = 0;
+    static constexpr int kMinCtas = 2;
+    static constexpr int kTmemCols = 1;
+    static constexpr int kGBytes = 4096;  // [hi, lo][K step 0, 1] x 1 KB
+    static constexpr int kWBytes = 2048;  // W tile per warp: 2 K steps x 1 KB
+    static __host__ __device__ constexpr size_t extra_bytes(int W) {
+        // G, W tiles, one mbarrier per warp, TMEM slot; at least the span an A operand reads (16 row groups of
+        // 256 B from the last G tile), so that the ignored rows never reach past this region
+        return ((std::max<size_t>((size_t)kGBytes + (size_t)W * kWBytes + (size_t)W * 8 + 128,
+                                  (size_t)3 * 1024 + 16 * 256 + 128)) +
+                127) /
+               128 * 128;
+    }
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)kGBytes + (size_t)W * kWBytes; }
+    uint32_t gbase, wt, d_tmem, ld_addr, ncommit, quarter_off;
+    uint64_t *mbar;
+    float *dx;
+    int cols, rows, batch, pend_col;
+    bool pending;
+
+    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int, int lane,
+                                         int W) {
+        const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+        gbase = smem_u32(extra);
+        wt = gbase + (uint32_t)kGBytes + (uint32_t)warp * (uint32_t)kWBytes;
+        mbar = reinterpret_cast<uint64_t *>(extra + kGBytes + (size_t)W * kWBytes) + warp;
+        if (lane == 0) mbar_init(mbar, 1);
+        fence_mbar_init();
+        __syncwarp();
+        quarter_off = (uint32_t)(warp & 3) * 1024u;  // 32 rows of A = 4 groups of 256 B
+        d_tmem = tmem_base + 32u * (uint32_t)warp;
+        ld_addr = d_tmem + (((uint32_t)(warp & 3) * 32u) << 16);
+        ncommit = 0;
+        pending = false;
+    }
+    __device__ __forceinline__ bool wait_mma(const Q8SLaunch &L) {
+        if (ncommit == 0) return true;
+        return mbar_wait_bounded(mbar, (ncommit - 1) & 1, L.status, L.spin_limit);
+    }
+    // CTA-wide (every warp calls it for the same item): G = s . dY of the stripe as bf16 hi/lo tiles
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int) {
+        const uint16_t *dy = reinterpret_cast<const uint16_t *>(J.x);
+        dx = J.ys;
+        cols = J.m.cols;
+        rows = J.m.rows;
+        batch = L.batch;
+        pending = false;
+        for (int t = threadIdx.x; t < 32 * 32; t += blockDim.x) {
+            const int v = t >> 5, r = t & 31;  // vector, stripe row
+            const int row = stripe * 32 + r;
+            float g = 0.f;
+            if (row < rows && v < batch)
+                g = J.scales[row] * __uint_as_float((uint32_t)__ldg(dy + (size_t)v * rows + row) << 16);
+            const __nv_bfloat16 h = __float2bfloat16_rn(g);
+            const __nv_bfloat16 l = __float2bfloat16_rn(g - __bfloat162float(h));
+            // K-major core matrices: vector group v/8 at 256 B, K half (r % 16) / 8 at 128 B, K step r / 16
+            const uint32_t off = (uint32_t)(r >> 4) * 1024u + (uint32_t)(v >> 3) * 256u +
+                                 (uint32_t)((r >> 3) & 1) * 128u + (uint32_t)(v & 7) * 16u + (uint32_t)(r & 7) * 2u;
+            asm volatile("st.shared.u16 [%0], %1;" ::"r"(gbase + off), "h"(__bfloat16_as_ushort(h)) : "memory");
+            asm volatile("st.shared.u16 [%0], %1;" ::"r"(gbase + 2048u + off), "h"(__bfloat16_as_ushort(l))
+                         : "memory");
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+    }
+    // add the finished D tile (vectors x 32 columns at pend_col) to dX
+    __device__ __forceinline__ void flush(const Q8SLaunch &L, int lane) {
+        wait_mma(L);
+        tcgen05_fence_after();
+        uint32_t r[32];
+        tmem_ld_32x32b_x32(ld_addr, r);  // lane = vector, r[j] = column pend_col + j
+        if (lane < batch) {
+            float *dst = dx + (size_t)lane * cols + pend_col;
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                if (pend_col + j < cols)  // cols % 16 == 0: a 4-column group inside the row stays inside
+                    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst + j),
+                                 "f"(__uint_as_float(r[j])), "f"(__uint_as_float(r[j + 1])),
+                                 "f"(__uint_as_float(r[j + 2])), "f"(__uint_as_float(r[j + 3]))
+                                 : "memory");
+        }
+        tcgen05_fence_before();
+        pending = false;
+    }
+    template <int ILP>
+    __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int,
+                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
+                                             int lane) {
+        const int qtot = (m.cols + 3) >> 2;
+        const int q0 = seg0 * m.seg_quads;
+        const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
+        if (nq <= 0) return;
+        const int npieces = (nq + 7) >> 3;
+        uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
+        const uint32_t kend = rows_now[0] * 32 + lane;
+        // lane = stripe row r: K step r / 16, K group (r / 8) % 2 (128 B), row r % 8 (16 B); N group g at 256 B
+        const uint32_t wdst = wt + (uint32_t)(lane >> 4) * 1024u + (uint32_t)((lane >> 3) & 1) * 128u +
+                              (uint32_t)(lane & 7) * 16u;
+        for (int p = 0; p < npieces; p++) {
+            uint32_t w[8];
+            decode_piece(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, P, w);
+            uint32_t a[16];
+#pragma unroll
+            for (int j = 0; j < 8; j++) i8x4_to_bf16x4(w[j], a[2 * j], a[2 * j + 1]);
+            if (pending) flush(L, lane);  // also: the previous MMAs are done with the W tile
+#pragma unroll
+            for (int g = 0; g < 4; g++)
+                asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(wdst + (uint32_t)g * 256u), "r"(a[4 * g]),
+                             "r"(a[4 * g + 1]), "r"(a[4 * g + 2]), "r"(a[4 * g + 3])
+                             : "memory");
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (elect_one()) {
+                tcgen05_fence_after();
+                const uint32_t idesc = umma_idesc_bf16(128, 32, 0, 1);
+#pragma unroll
+                for (int kk = 0; kk < 2; kk++) {
+                    const uint64_t bd = umma_smem_desc(wt + (uint32_t)kk * 1024u, 128u, 256u);
+                    const uint32_t ga = gbase + (uint32_t)kk * 1024u - quarter_off;
+                    umma_f16_ss(d_tmem, umma_smem_desc(ga, 128u, 256u), bd, idesc, kk ? 1u : 0u);
+                    umma_f16_ss(d_tmem, umma_smem_desc(ga + 2048u, 128u, 256u), bd, idesc, 1u);
+                }
+                umma_commit(mbar);
+            }
+            __syncwarp();
+            ncommit++;
+            pending = true;
+            pend_col = 4 * q0 + 32 * p;
+        }
+        if (hi != 0 || lo != P) atomicOr(L.status, MV_DEV_FINAL_STATE);
+    }
+    __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &, int, int, int lane, int, void *) {
+        if (pending) flush(L, lane);
+        __syncthreads();  // G and the W tiles are rewritten by the next item
+    }
+    __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_mma(L); }
+};
+
 template <class Cons, int ILP, int DEPTH>
 __global__ void __launch_bounds__(256, Cons::kMinCtas) q8s_kernel(const Q8SLaunch L) {
     constexpr int NV = Cons::kRedNV;
@@ -959,7 +1303,17 @@ mv_status launch_q8s(const Q8SLaunch &L, int nv, const mv_q8_tuning &t, cudaStre
 }
 
 // mode 1: float forward, mode 2: float backward (transposed); nv in {1,2,4,8}
-mv_status launch_q8f(const Q8SLaunch &L, int mode, int nv, const mv_q8_tuning &t, cudaStream_t st) {
+// float form: batches of at least this many vectors go to the tensor-core consumers (engine 0)
+constexpr int kFloatMmaMinBatch = 2;
+
+// vectors per pass of the float form: the tensor-core consumers take 16 (forward) / 32 (backward)
+int q8f_pass(int mode, int batch, const mv_q8_tuning &t) {
+    if (t.engine == MV_ENGINE_AUTO && batch >= kFloatMmaMinBatch) return mode == 1 ? FwdMma::kNV : BwdMma::kNV;
+    return 8;
+}
+
+mv_status launch_q8f(const Q8SLaunch &L, int mode, int nv, const mv_q8_tuning &t, bool mma, cudaStream_t st) {
+    if (mma) return mode == 1 ? launch_q8s_c<FwdMma>(L, t, st) : launch_q8s_c<BwdMma>(L, t, st);
     if (mode == 1) {
         switch (nv) {
             case 1: return launch_q8s_c<FwdCons<1>>(L, t, st);
@@ -1061,8 +1415,10 @@ mv_status q8f_run(const mv_q8_view *m, int mode, const uint16_t *in, int batch, 
     const int in_len = mode == 1 ? m->cols : m->rows;   // elements per vector in
     const int out_len = mode == 1 ? m->rows : m->cols;  // elements per vector out
     if (mode == 2) MV_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)batch * out_len, st), "memset(dx)");
-    for (int v0 = 0; v0 < batch; v0 += 8) {
-        const int nb = std::min(8, batch - v0);
+    const int pass = q8f_pass(mode, batch, t);
+    const bool mma = pass > 8;
+    for (int v0 = 0; v0 < batch; v0 += pass) {
+        const int nb = std::min(pass, batch - v0);
         Q8SLaunch L{};
         L.job0.m = *m;
         L.job0.x = reinterpret_cast<const int8_t *>(in + (size_t)v0 * in_len);
@@ -1088,7 +1444,7 @@ mv_status q8f_run(const mv_q8_view *m, int mode, const uint16_t *in, int batch, 
         L.buf_words = (m->max_blk_rows + 1) * 32;
         L.tbl_stage = (int)((m->tbl_stripe_max + 7) & ~7u);
         L.lut_stride = 32;
-        rc = launch_q8f(L, mode, nv_round(nb), t, st);
+        rc = launch_q8f(L, mode, nv_round(nb), t, mma, st);
         if (rc) return rc;
     }
     return MV_OK;
