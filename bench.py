@@ -273,6 +273,14 @@ def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, r
 
         t_dense, gd = time_graph(torch, dense_step, reps)
         del gd
+        t_gemm = None
+        if B % 8 == 0:
+            xts = [x.t() for x in xs]
+            t_gemm, gg = time_graph(torch, lambda: [torch._int_mm(m["Wd"], xt) for m, xt in zip(mats, xts)], reps)
+            del gg
+            for m, xt, yr in zip(mats, xts, ref):
+                if not torch.equal(torch._int_mm(m["Wd"], xt).t(), yr):
+                    raise SystemExit(f"bench: cuBLAS int8 GEMM disagrees with dense dp4a on {m['spec']['name']}")
         cands = autotune.candidates_for(B, autotune.CANDIDATES)
         best, res = autotune.tune_stack(lambda t: ops.Q8Stack(Ms, batch=B, tuning=t, xs=xs, device=dev),
                                         candidates=cands, reps=reps)
@@ -300,10 +308,89 @@ def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, r
         row["candidates_us"] = {k: round(v, 1) for k, v in sorted(res.items(), key=lambda kv: kv[1])}
         row["dense_dp4a_us_per_step"] = round(1e3 * t_dense, 1)
         row["speedup_vs_dense_dp4a"] = round(1e3 * t_dense / fastest["us_per_step"], 3)
+        row["cublas_int8_gemm_us_per_step"] = None if t_gemm is None else round(1e3 * t_gemm, 1)
+        row["speedup_vs_cublas_int8_gemm"] = None if t_gemm is None else round(1e3 * t_gemm / fastest["us_per_step"], 3)
         out["batches"][f"B{B}"] = row
         del xs, ref
     del mats, Ms
     torch.cuda.empty_cache()
+    ops.device_status()
+    return out
+
+
+# ------------------------------------------------------------------ large low-entropy matrices
+
+LARGE_SHAPES = [(16384, 16384), (28672, 8192)]
+LARGE_DISTS = [("laplace_b2", None), ("normal_s1", 1.0)]
+
+
+def gen_large(torch, shape, dist, seed, dev):
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    if dist == "laplace_b2":
+        z = 2.0 * (torch.empty(shape, device=dev).exponential_(generator=g) -
+                   torch.empty(shape, device=dev).exponential_(generator=g))
+    else:
+        z = torch.randn(shape, device=dev, generator=g)
+    return torch.clamp(torch.round(z), -127, 127).to(torch.int8)
+
+
+def int8_gemm_us(torch, Ws, x, reps=10):
+    """cuBLAS int8 tensor-core GEMM (torch._int_mm, exact int32) y^T = W x^T over rotating copies of W, in us
+    per matrix; None where its shape rules (> 16 rows, columns and vectors in multiples of 8) exclude it."""
+    B, cols = x.shape
+    if B % 8 or cols % 8 or Ws[0].shape[0] <= 16:
+        return None
+    xt = x.t()  # [cols, B], column-major
+    try:
+        t, _ = time_graph(torch, lambda: [torch._int_mm(w, xt) for w in Ws], reps, inner=len(Ws))
+    except RuntimeError:
+        return None
+    return 1e3 * t
+
+
+def large_section(torch, ops, autotune, dev, batches=(1, 16)):
+    """configs: 16384x16384 and 28672x8192, Laplace(b=2) and round(N(0,1)), per-row tables, B in {1, 16}:
+    us per matvec of the autotuned single launch and of dense dp4a, bits/weight vs entropy, HBM GB/s."""
+    from matvans_b200 import codec
+    out = {}
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5)
+    for i, shape in enumerate(LARGE_SHAPES):
+        for j, (dist, _) in enumerate(LARGE_DISTS):
+            Wd = gen_large(torch, shape, dist, 4000 + 10 * i + j, dev)
+            M = ops.Q8Matrix(codec.q8_encode(Wd.cpu().numpy(), local=True), dev)
+            rows, cols = shape
+            row = {"bits_per_weight": round(M.bits_per_weight, 3), "entropy_bits": round(entropy_dev(torch, Wd), 3),
+                   "compressed_bytes": M.payload_bytes}
+            Ws = [Wd] + [Wd.clone() for _ in range(copies_for(rows * cols) - 1)]
+            for B in batches:
+                x = torch.randint(-127, 128, (B, cols), dtype=torch.int8, device=dev, generator=gen)
+                yd = torch.empty((B, rows), dtype=torch.int32, device=dev)
+                t_dense, _ = time_graph(torch, lambda: [ops.dense_matvec(w, x, out=yd) for w in Ws], 10, inner=len(Ws))
+                tun, info = autotune.tune(M, batch=B)
+                y = M.matvec(x, tuning=tun)
+                ops.dense_matvec(Wd, x, out=yd)
+                torch.cuda.synchronize()
+                if not torch.equal(y, yd):
+                    raise SystemExit(f"bench: large {shape} {dist} B={B} is not bit-exact")
+                us = info["us"]
+                alg = M.payload_bytes + B * cols + 4 * B * rows
+                gemm = int8_gemm_us(torch, Ws, x)
+                if gemm is not None:
+                    ref = torch._int_mm(Wd, x.t()).t()
+                    if not torch.equal(ref, yd):
+                        raise SystemExit(f"bench: cuBLAS int8 GEMM disagrees with dense dp4a on {shape} {dist}")
+                row[f"B{B}"] = {"us": round(us, 2), "dense_dp4a_us": round(1e3 * t_dense, 2),
+                                "speedup_vs_dense_dp4a": round(1e3 * t_dense / us, 3),
+                                "cublas_int8_gemm_us": None if gemm is None else round(gemm, 2),
+                                "speedup_vs_cublas_int8_gemm": None if gemm is None else round(gemm / us, 3),
+                                "int8_equiv_gbs": round(int8_equiv_bytes(rows, cols, B) / us / 1e3, 1),
+                                "compressed_gbs": round(alg / us / 1e3, 1),
+                                "tuning": [tun.warps, tun.ilp, tun.depth, tun.ctas_per_sm, tun.parts, tun.engine]}
+            out[f"{rows}x{cols}_{dist}"] = row
+            del Ws, Wd, M
+            torch.cuda.empty_cache()
     ops.device_status()
     return out
 
@@ -489,6 +576,7 @@ def run_ours(args):
     ops.device_status()
 
     stack224 = None if args.no_stack else stack_section(torch, ops, autotune, dev)
+    large = None if args.no_stack else large_section(torch, ops, autotune, dev)
 
     # end to end through the public API: pinned host x in, int32 y out, every step
     xh = {c: torch.from_numpy(v).pin_memory() for c, v in x_by_cols.items()}
@@ -541,6 +629,7 @@ def run_ours(args):
             "warp_per_row_kernel": wpr_t,
             "float_form": float_form,
             "stack224": stack224,
+            "large_low_entropy": large,
             "speedup_vs_dense_dp4a": {k: round(dense[k.split("_s")[0]]["us"] / v["us"], 3)
                                       for k, v in per.items() if k.split("_s")[0] in dense and "_s4_" in k},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -593,7 +682,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-stack", action="store_true", help="skip the 224-matrix batched stack section")
+    ap.add_argument("--no-stack", action="store_true",
+                    help="skip the 224-matrix batched stack and the large low-entropy sections")
     ap.add_argument("--profile-stack", default="",
                     help="LAYERS,B,ENGINE[,WARPS]: build a stack of LAYERS x 7 matrices and run two steps at B "
                          "vectors with the given engine and warps per CTA (the case ncu captures)")

@@ -16,18 +16,29 @@
 
 namespace mv {
 
-template <int NV>
+// x chunk i of vector v: staged in shared memory, or (XG, when NV x cols does not fit) read through
+// L1/L2, where every warp of the GPU reads the same few hundred KB
+template <int NV, bool XG>
+__device__ __forceinline__ uint4 x_chunk(const uint4 *xs, const uint4 *xg, int v, int chunks, int i, int batch) {
+    if (XG) return v < batch ? __ldg(xg + (size_t)v * chunks + i) : make_uint4(0, 0, 0, 0);
+    return xs[v * chunks + i];
+}
+
+template <int NV, bool XG>
 __global__ void __launch_bounds__(256) dense_kernel(const int8_t *__restrict__ W, int rows, int cols,
                                                     const int8_t *__restrict__ x, int batch,
                                                     int32_t *__restrict__ y) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint4 *xs = reinterpret_cast<uint4 *>(smem);  // [NV][cols/16]
+    uint4 *xs = reinterpret_cast<uint4 *>(smem);  // [NV][cols/16] unless XG
+    const uint4 *xg = reinterpret_cast<const uint4 *>(x);
     const int chunks = cols >> 4;
-    for (int i = threadIdx.x; i < NV * chunks; i += blockDim.x) {
-        const int v = i / chunks;
-        xs[i] = v < batch ? reinterpret_cast<const uint4 *>(x)[i] : make_uint4(0, 0, 0, 0);
+    if (!XG) {
+        for (int i = threadIdx.x; i < NV * chunks; i += blockDim.x) {
+            const int v = i / chunks;
+            xs[i] = v < batch ? xg[i] : make_uint4(0, 0, 0, 0);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int row = blockIdx.x * nw + warp; row < rows; row += gridDim.x * nw) {
         const uint4 *wr = reinterpret_cast<const uint4 *>(W + (size_t)row * cols);
@@ -43,7 +54,7 @@ __global__ void __launch_bounds__(256) dense_kernel(const int8_t *__restrict__ W
             for (int u = 0; u < 4; u++)
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
-                    const uint4 b = xs[v * chunks + i + 32 * u];
+                    const uint4 b = x_chunk<NV, XG>(xs, xg, v, chunks, i + 32 * u, batch);
                     acc[v] = __dp4a((int)a[u].x, (int)b.x, acc[v]);
                     acc[v] = __dp4a((int)a[u].y, (int)b.y, acc[v]);
                     acc[v] = __dp4a((int)a[u].z, (int)b.z, acc[v]);
@@ -54,7 +65,7 @@ __global__ void __launch_bounds__(256) dense_kernel(const int8_t *__restrict__ W
             const uint4 a = ldg_nc_u4(wr + i);
 #pragma unroll
             for (int v = 0; v < NV; v++) {
-                const uint4 b = xs[v * chunks + i];
+                const uint4 b = x_chunk<NV, XG>(xs, xg, v, chunks, i, batch);
                 acc[v] = __dp4a((int)a.x, (int)b.x, acc[v]);
                 acc[v] = __dp4a((int)a.y, (int)b.y, acc[v]);
                 acc[v] = __dp4a((int)a.z, (int)b.z, acc[v]);
@@ -78,9 +89,9 @@ template <int NV>
 mv_status launch_dense(const int8_t *W, int rows, int cols, const int8_t *x, int batch, int32_t *y,
                        cudaStream_t st) {
     const int nw = 8;
-    const size_t smem = (size_t)NV * cols;
-    if (smem > (size_t)max_smem_optin()) return fail(MV_ERR_UNSUPPORTED, "dense: x does not fit shared memory");
-    auto kern = dense_kernel<NV>;
+    const bool xg = (size_t)NV * cols > (size_t)max_smem_optin();
+    const size_t smem = xg ? 0 : (size_t)NV * cols;
+    auto kern = xg ? dense_kernel<NV, true> : dense_kernel<NV, false>;
     int bps = 0;
     mv_status rc = prepare_kernel((const void *)kern, smem, 32 * nw, &bps);
     if (rc) return rc;
@@ -189,8 +200,12 @@ mv_status dense_matvec(const int8_t *W, int rows, int cols, const int8_t *x, int
     if (cols % 16) return fail(MV_ERR_SHAPE, "mv_dense_matvec: cols %% 16 != 0");
     if (((uintptr_t)W & 15) || ((uintptr_t)x & 15))
         return fail(MV_ERR_ARG, "mv_dense_matvec: W and x must be 16-byte aligned");
-    for (int v0 = 0; v0 < batch; v0 += 16) {
-        const int nb = std::min(16, batch - v0);
+    // vectors per pass: up to 16, fewer when their x does not fit shared memory (x is then read through the
+    // caches only if a single vector does not fit)
+    int pass = 16;
+    while (pass > 1 && (size_t)pass * cols > (size_t)max_smem_optin()) pass >>= 1;
+    for (int v0 = 0; v0 < batch; v0 += pass) {
+        const int nb = std::min(pass, batch - v0);
         const int8_t *xv = x + (size_t)v0 * cols;
         int32_t *yv = y + (size_t)v0 * rows;
         mv_status rc;

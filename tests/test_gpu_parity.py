@@ -232,6 +232,14 @@ def test_dense_comparator():
             x = rnd_x(rng, B, shape[1])
             assert np.array_equal(ops.dense_matvec(Wd, torch.from_numpy(x)).cpu().numpy(),
                                   oracle.matvec_i8(W, x))
+    # 16 vectors x 16384 columns exceed shared memory (passes of 8); 300000 columns exceed it for one
+    # vector (x read through the caches)
+    for cols in (16384, 300000):
+        W = gauss(rng, 2.0, (40, cols))
+        Wd = torch.from_numpy(W).cuda()
+        for B in (1, 9, 16):
+            x = rnd_x(rng, B, cols)
+            assert np.array_equal(ops.dense_matvec(Wd, torch.from_numpy(x)).cpu().numpy(), oracle.matvec_i8(W, x))
 
 
 # -------------------------------------------------- device-side error paths
