@@ -650,6 +650,58 @@ def run_ours(args):
     return 0
 
 
+def run_profile_kernel(args):
+    """Small fixed case of one kernel family for ncu: a bit-exact (or FP64-checked) gate, then two plain
+    launches of each kernel.  awr / wpr / dense: 4096x4096 sigma 4, B = 1 (dense also B = 16);
+    float: 11008x4096 sigma 4, per-row tables, B = 64 forward and backward on the tensor cores."""
+    import torch
+    from matvans_b200 import ops
+    import oracle
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(11)
+    if args.profile_kernel == "float":
+        shape = (11008, 4096)
+        W = gen_matrix(shape, 4.0, 21)
+        M = ops.Q8Matrix.encode(W, local=True, device=dev)
+        s = rng.uniform(1e-3, 1e-2, shape[0]).astype(np.float32)
+        st = torch.from_numpy(s).to(dev)
+        X = torch.from_numpy(rng.standard_normal((64, shape[1])).astype(np.float32)).to(torch.bfloat16).to(dev)
+        dY = torch.from_numpy(rng.standard_normal((64, shape[0])).astype(np.float32)).to(torch.bfloat16).to(dev)
+        Y = M.matvec_bf16(X, st).double()
+        Wd = torch.from_numpy(W).to(dev).double()
+        ref = (X.double() @ Wd.T) * st.double()[None, :]
+        if not torch.allclose(Y, ref, rtol=1e-4, atol=1e-4 * ref.abs().max().item()):
+            raise SystemExit("bench: float forward disagrees with the FP64 product")
+        for _ in range(2):
+            M.matvec_bf16(X, st)
+            M.matvec_t_bf16(dY, st)
+    else:
+        shape = (4096, 4096)
+        W = gen_matrix(shape, 4.0, 22)
+        x = rng.integers(-127, 128, size=(1, shape[1])).astype(np.int8)
+        xd = torch.from_numpy(x).to(dev)
+        yref = oracle.matvec_i8(W, x)
+        if args.profile_kernel == "awr":
+            A = ops.AwrMatrix.encode(W, device=dev)
+            run = lambda: A.matvec(xd)
+        elif args.profile_kernel == "wpr":
+            P = ops.WprMatrix.encode(W, device=dev)
+            run = lambda: P.matvec(xd)
+        else:
+            Wd = torch.from_numpy(W).to(dev)
+            x16 = torch.from_numpy(rng.integers(-127, 128, size=(16, shape[1])).astype(np.int8)).to(dev)
+            if not np.array_equal(ops.dense_matvec(Wd, x16).cpu().numpy(), oracle.matvec_i8(W, x16.cpu().numpy())):
+                raise SystemExit("bench: dense B=16 is not bit-exact")
+            run = lambda: (ops.dense_matvec(Wd, xd), ops.dense_matvec(Wd, x16))[0]
+        if not np.array_equal(run().cpu().numpy().reshape(1, -1), yref.reshape(1, -1)):
+            raise SystemExit(f"bench: {args.profile_kernel} is not bit-exact")
+        for _ in range(2):
+            run()
+    torch.cuda.synchronize()
+    ops.device_status()
+    return 0
+
+
 def run_profile_stack(args):
     """Small fixed stack case for ncu: gate + two plain steps."""
     import torch
@@ -684,6 +736,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stack", action="store_true",
                     help="skip the 224-matrix batched stack and the large low-entropy sections")
+    ap.add_argument("--profile-kernel", default="", choices=["", "awr", "wpr", "dense", "float"],
+                    help="small fixed case of one kernel family (the case ncu captures)")
     ap.add_argument("--profile-stack", default="",
                     help="LAYERS,B,ENGINE[,WARPS]: build a stack of LAYERS x 7 matrices and run two steps at B "
                          "vectors with the given engine and warps per CTA (the case ncu captures)")
@@ -696,6 +750,8 @@ def main():
         return run_reference(args)
     if args.profile_stack:
         return run_profile_stack(args)
+    if args.profile_kernel:
+        return run_profile_kernel(args)
     return run_ours(args)
 
 
