@@ -154,8 +154,31 @@ static mv_status q8_encode(const int8_t *W, int rows, int cols, int local, int s
     e.qtot = (cols + 3) / 4;
     e.stripes = (rows + 31) / 32;
     e.local = local != 0;
-    if (seg_quads <= 0) {
-        // segments of 32..64 quads (a multiple of 4), as many as it takes to give
+    if (seg_quads <= 0 && e.stripes >= 64 && e.qtot > 64) {
+        // enough stripes to fill the GPU with whole-stripe work items: segments of 32..64 quads (a multiple
+        // of 4) that the 4 or 8 warps of a CTA share most evenly (a stripe ends in a CTA barrier, so its
+        // slowest warp sets its time), with a small preference for longer segments (fewer coder states)
+        double best = -1.0;
+        for (int sq = 64; sq >= 32; sq -= 4) {
+            const int n = (e.qtot + sq - 1) / sq, last = e.qtot - (n - 1) * sq;
+            double eff = 1.0;
+            for (int W : {4, 8}) {
+                int worst = 0;
+                for (int w = 0; w < W && w < n; w++) {
+                    int work = 0;
+                    for (int g = w; g < n; g += W) work += (g == n - 1) ? last : sq;
+                    worst = std::max(worst, work);
+                }
+                eff = std::min(eff, (double)e.qtot / ((double)W * worst));
+            }
+            const double score = eff * (1.0 - 0.1 * 16.0 / sq);
+            if (score > best + 1e-9) {
+                best = score;
+                seg_quads = sq;
+            }
+        }
+    } else if (seg_quads <= 0) {
+        // few stripes: segments of 32..64 quads (a multiple of 4), as many as it takes to give
         // 148 SMs x 16 warps at least one (stripe, segment) each
         int64_t want = (2368 + e.stripes - 1) / e.stripes;
         int64_t lo = (e.qtot + 63) / 64, hi = std::max(1, e.qtot / 32);
