@@ -231,6 +231,22 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
 mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info,
                              int batch, const mv_q8_tuning *tuning, void *stream);
 
+/* Chained pipeline, the reference's end-to-end workload (buffered/ans-warp-rows.cu:208-221:
+ * int32 y -> fp32 scale -> int8 -> next matrix), fused into one persistent,
+ * cooperative launch.  jobs[j+1].x receives clamp(round_half_even((float)y_j[r] *
+ * chain_scales[j]), -128, 127) for every row r of job j (the requantisation of
+ * ans-warp-rows-kernel.cu:212-220); the last job's goes to out8 [batch][rows].
+ * jobs[0].x is the input; y_j (int32) and, with scales, ys_j are written as in a stack.
+ * Work items of job j+1 wait (bounded) until every item of job j is done;
+ * jobs[j].pad is the device-side counter (reset by each call).  Plan with
+ * mv_q8_chain_plan (checks rows_j == cols_{j+1}, whole stripes).  jobs_dev is
+ * modified (the counters); concurrent calls on the same jobs_dev race. */
+mv_status mv_q8_chain_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning,
+                           mv_q8_stack_info *info);
+mv_status mv_q8_chain_matvec(mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info, int batch,
+                             const float *chain_scales_dev, int8_t *out8_dev,
+                             const mv_q8_tuning *tuning, void *stream);
+
 /* Float form (no reference counterpart): y[b][r] = s[r] * sum_c W[r][c] *
  * x[b][c] with x bf16 [batch][cols] (16-byte aligned), fp32 accumulation in a
  * fixed order (deterministic), fp32 y [batch][rows].  cols % 16 == 0.  Passes

@@ -24,7 +24,7 @@ EXPORTS = [
     "mv_dense_matvec", "mv_blob_free", "mv_blob_get", "mv_blob_get_i64", "mv_blob_name", "mv_awr_encode",
     "mv_wpr_encode", "mv_q8_encode", "mv_read_safetensors", "mv_write_safetensors", "mv_read_wpr_bin",
     "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc", "mv_q8_matvec_tuned", "mv_q8_stack_plan",
-    "mv_q8_stack_matvec", "mv_q8_matvec_bf16", "mv_q8_matvec_t_bf16",
+    "mv_q8_stack_matvec", "mv_q8_matvec_bf16", "mv_q8_matvec_t_bf16", "mv_q8_chain_plan", "mv_q8_chain_matvec",
 ]
 
 
@@ -89,6 +89,8 @@ def lib():
         "mv_q8_matvec_tuned": ([ctypes.POINTER(Q8View), P, i32, P, P, P, ctypes.POINTER(Q8Tuning), P], st),
         "mv_q8_stack_plan": ([ctypes.POINTER(Q8Job), i32, ctypes.POINTER(Q8Tuning), ctypes.POINTER(Q8StackInfo)], st),
         "mv_q8_stack_matvec": ([P, i32, ctypes.POINTER(Q8StackInfo), i32, ctypes.POINTER(Q8Tuning), P], st),
+        "mv_q8_chain_plan": ([ctypes.POINTER(Q8Job), i32, ctypes.POINTER(Q8Tuning), ctypes.POINTER(Q8StackInfo)], st),
+        "mv_q8_chain_matvec": ([P, i32, ctypes.POINTER(Q8StackInfo), i32, P, P, ctypes.POINTER(Q8Tuning), P], st),
         "mv_q8_matvec_bf16": ([ctypes.POINTER(Q8View), P, i32, P, P, ctypes.POINTER(Q8Tuning), P], st),
         "mv_q8_matvec_t_bf16": ([ctypes.POINTER(Q8View), P, i32, P, P, ctypes.POINTER(Q8Tuning), P], st),
         "mv_dense_matvec": ([P, i32, i32, P, i32, P, P], st),

@@ -55,6 +55,10 @@ struct Q8SLaunch {
     int buf_words;       // per segment buffer, u32 words
     int tbl_stage;       // staged table entries
     uint32_t lut_stride; // 32 (words per quantile row of the table); a runtime value on purpose
+    // chained pipeline (mv_q8_chain_matvec): job j's int8 output clamp(rn(y * chain_scales[j])) is job
+    // j+1's x (the last job's goes to chain_out8); jobs[j].pad counts job j's finished work items
+    const float *chain_scales;
+    int8_t *chain_out8;
 };
 
 struct ItemInfo {
@@ -150,18 +154,45 @@ __device__ __forceinline__ void issue_step(const Q8SLaunch &L, const StepCursor 
     }
 }
 
+// x loads: through the read-only path, or (coh: x was written earlier in the same launch, by the
+// chained pipeline) through L2 only
+__device__ __forceinline__ uint4 ldx_u4(const void *p, bool coh) {
+    if (coh) {
+        uint4 v;
+        asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+        return v;
+    }
+    return __ldg(reinterpret_cast<const uint4 *>(p));
+}
+__device__ __forceinline__ uint32_t ldx_u32(const void *p, bool coh) {
+    if (coh) {
+        uint32_t v;
+        asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(p));
+        return v;
+    }
+    return __ldg(reinterpret_cast<const uint32_t *>(p));
+}
+
 template <int NV>
-__device__ __forceinline__ void load_x(const int8_t *x, int cols, int q, uint32_t (&xv)[NV]) {
+__device__ __forceinline__ void load_x(const int8_t *x, int cols, int q, uint32_t (&xv)[NV], bool coh) {
 #pragma unroll
-    for (int v = 0; v < NV; v++)
-        xv[v] = __ldg(reinterpret_cast<const uint32_t *>(x + (size_t)v * cols) + q);
+    for (int v = 0; v < NV; v++) xv[v] = ldx_u32(reinterpret_cast<const uint32_t *>(x + (size_t)v * cols) + q, coh);
 }
 
 // Four consecutive quads of x (16 bytes) per vector; q % 4 == 0.
 template <int NV>
-__device__ __forceinline__ void load_x4(const int8_t *x, int cols, int q, uint4 (&xv)[NV]) {
+__device__ __forceinline__ void load_x4(const int8_t *x, int cols, int q, uint4 (&xv)[NV], bool coh) {
 #pragma unroll
-    for (int v = 0; v < NV; v++) xv[v] = __ldg(reinterpret_cast<const uint4 *>(x + (size_t)v * cols + 4 * q));
+    for (int v = 0; v < NV; v++) xv[v] = ldx_u4(x + (size_t)v * cols + 4 * q, coh);
+}
+
+// The chained pipeline's epilogue of one output: job j's int8 result, the reference's fp32
+// requantisation (ans-warp-rows-kernel.cu:212-220), stored as the next job's x.
+__device__ __forceinline__ void chain_emit(const Q8SLaunch &L, const Q8Job &J, int v, int row, int sum) {
+    const int j = (int)(&J - L.jobs);
+    const int r = __float2int_rn((float)sum * __ldg(L.chain_scales + j));
+    int8_t *o = j + 1 < L.njobs ? const_cast<int8_t *>(L.jobs[j + 1].x) : L.chain_out8;
+    o[(size_t)v * J.m.rows + row] = (int8_t)max(-128, min(127, r));
 }
 
 template <int NV>
@@ -225,21 +256,23 @@ struct IntCons {
                                              int lane);
     const int8_t *x;
     int cols;
+    bool coh;
     int acc[NV];
     struct Group {
         uint4 xv[NV];
     };
-    __device__ __forceinline__ void begin_item(const Q8SLaunch &, const Q8Job &J, int, int) {
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
         x = J.x;
         cols = J.m.cols;
+        coh = L.chain_scales != nullptr;
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = 0;
     }
-    __device__ __forceinline__ void load_group(Group &g, int q) const { load_x4<NV>(x, cols, q, g.xv); }
+    __device__ __forceinline__ void load_group(Group &g, int q) const { load_x4<NV>(x, cols, q, g.xv, coh); }
     __device__ __forceinline__ void use(const Group &g, int j, int, uint32_t wq, int) { dot4<NV>(wq, g.xv, j, acc); }
     __device__ __forceinline__ void single(int q, uint32_t wq, int) {
         uint32_t xv[NV];
-        load_x<NV>(x, cols, q, xv);
+        load_x<NV>(x, cols, q, xv, coh);
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wq, (int)xv[v], acc[v]);
     }
@@ -262,6 +295,7 @@ struct IntCons {
                 } else {
                     *dst = sum;
                     if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
+                    if (L.chain_scales) chain_emit(L, J, v, row, sum);
                 }
             }
         }
@@ -553,7 +587,7 @@ struct MmaCons {
     int *xbase;
     const int8_t *x;
     int cols, batch;
-    bool any;
+    bool any, coh;
 
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int,
                                          int lane, int W) {
@@ -581,6 +615,7 @@ struct MmaCons {
         cols = J.m.cols;
         batch = L.batch;
         any = false;
+        coh = L.chain_scales != nullptr;
     }
     // wait until every MMA issued so far completed (the latest commit covers all earlier MMAs)
     __device__ __forceinline__ bool wait_mma(const Q8SLaunch &L) {
@@ -610,8 +645,7 @@ struct MmaCons {
             const int c = pbase + i;
             xr[i] = make_uint4(0, 0, 0, 0);
             // cols % 16 == 0, so a 16-byte piece that starts inside the row ends inside it
-            if (xok && c < npieces && colbase + 32 * c < cols)
-                xr[i] = __ldg(reinterpret_cast<const uint4 *>(xrow + 32 * c));
+            if (xok && c < npieces && colbase + 32 * c < cols) xr[i] = ldx_u4(xrow + 32 * c, coh);
         }
     }
     template <int ILP>
@@ -708,6 +742,7 @@ struct MmaCons {
                 } else {
                     *dst = sum;
                     if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
+                    if (L.chain_scales) chain_emit(L, J, v, row, sum);
                 }
             }
         }
@@ -1058,6 +1093,31 @@ struct BwdMma {
     __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_mma(L); }
 };
 
+// Chained pipeline: wait (one thread, bounded, then the whole CTA) until every work item of job j is
+// counted.  Work items are numbered in job order and each CTA takes its items in increasing order, and
+// the launch is cooperative (all CTAs resident), so the items waited for are always making progress.
+__device__ __forceinline__ void chain_wait(const Q8SLaunch &L, int j) {
+    if (threadIdx.x == 0) {
+        const uint32_t need = (j + 1 < L.njobs ? L.jobs[j + 1].item0 : L.nitems) - L.jobs[j].item0;
+        const uint32_t *cnt = &L.jobs[j].pad;
+        for (uint32_t it = 0;; it++) {
+            uint32_t done;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(done) : "l"(cnt) : "memory");
+            if (done >= need) break;
+            if (it >= L.spin_limit) {
+                atomicOr(L.status, MV_DEV_WAIT_TIMEOUT);
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void q8s_chain_reset(Q8Job *jobs, int njobs) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x) jobs[j].pad = 0;
+}
+
 template <class Cons, int ILP, int DEPTH>
 __global__ void __launch_bounds__(256, Cons::kMinCtas) q8s_kernel(const Q8SLaunch L) {
     constexpr int NV = Cons::kRedNV;
@@ -1158,6 +1218,7 @@ __global__ void __launch_bounds__(256, Cons::kMinCtas) q8s_kernel(const Q8SLaunc
             lut_stripe = I.stripe;
         }
 
+        if (L.chain_scales && I.job > 0) chain_wait(L, I.job - 1);
         cons.begin_item(L, J, I.stripe, lane);
         const int steps = warp_steps(send - sbeg, warp, W, ILP);
         for (int j = 0; j < steps; j++) {
@@ -1190,7 +1251,11 @@ __global__ void __launch_bounds__(256, Cons::kMinCtas) q8s_kernel(const Q8SLaunc
             __syncwarp();
         }
 
-        cons.finish_item(L, J, I.stripe, warp, lane, W, red);
+        cons.finish_item(L, J, I.stripe, warp, lane, W, red);  // ends with a CTA barrier
+        if (L.chain_scales && threadIdx.x == 0) {
+            __threadfence();  // this item's outputs are visible before it is counted
+            atomicAdd(const_cast<uint32_t *>(&L.jobs[I.job].pad), 1u);
+        }
     }
     if (Cons::kTmemCols) {
         cons.drain(L);
@@ -1269,6 +1334,18 @@ mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t 
         if (rc) return rc;
         if (ctas_per_sm > 0) bps = std::min(bps, ctas_per_sm);
         bps = std::max(1, std::min<int>(bps, 512 / MmaCons::tmem_cols(W)));
+    }
+    if (L.chain_scales) {
+        // the chained pipeline waits across CTAs: a cooperative launch guarantees that they are all resident
+        int coop = 0;
+        MV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&coop, kern, 32 * W, smem), "occupancy");
+        coop = std::max(1, std::min(coop, bps));
+        const long long grid = std::max(1LL, std::min<long long>(L.nitems, (long long)coop * sm_count()));
+        Q8SLaunch Lc = L;
+        void *args[] = {&Lc};
+        MV_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)kern, dim3((unsigned)grid), dim3(32 * W), args, smem, st),
+                    "q8 chain cooperative launch");
+        return MV_OK;
     }
     const long long grid = std::max(1LL, std::min<long long>(L.nitems, (long long)bps * sm_count()));
     kern<<<(unsigned)grid, 32 * W, smem, st>>>(L);
@@ -1499,6 +1576,48 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
     info->ilp = t.ilp;
     info->depth = t.depth;
     return MV_OK;
+}
+
+mv_status mv_q8_chain_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning, mv_q8_stack_info *info) {
+    if (!jobs || njobs <= 0 || !info) return mv::fail(MV_ERR_ARG, "mv_q8_chain_plan: bad arguments");
+    for (int j = 0; j + 1 < njobs; j++)
+        if (jobs[j].m.rows != jobs[j + 1].m.cols)
+            return mv::fail(MV_ERR_SHAPE, "mv_q8_chain_plan: job %d has %d rows but job %d has %d columns", j,
+                            jobs[j].m.rows, j + 1, jobs[j + 1].m.cols);
+    mv_q8_tuning t = mv::resolve(tuning);
+    if (t.parts > 1) return mv::fail(MV_ERR_ARG, "mv_q8_chain_plan: a chain needs whole stripes (parts <= 1)");
+    t.parts = 0;
+    return mv_q8_stack_plan(jobs, njobs, &t, info);
+}
+
+mv_status mv_q8_chain_matvec(mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info, int batch,
+                             const float *chain_scales_dev, int8_t *out8_dev, const mv_q8_tuning *tuning,
+                             void *stream) {
+    if (!jobs_dev || njobs <= 0 || !info || batch <= 0 || batch > 16 || !chain_scales_dev || !out8_dev)
+        return mv::fail(MV_ERR_ARG, "mv_q8_chain_matvec: bad arguments (batch must be 1..16)");
+    mv_q8_tuning t = mv::resolve(tuning);
+    if (t.parts > 1) return mv::fail(MV_ERR_ARG, "mv_q8_chain_matvec: a chain needs whole stripes (parts <= 1)");
+    if (t.warps != info->warps || t.ilp != info->ilp)
+        return mv::fail(MV_ERR_ARG, "mv_q8_chain_matvec: tuning differs from the one the jobs were planned with");
+    cudaStream_t st = (cudaStream_t)stream;
+    mv_status rc;
+    mv::Q8SLaunch L{};
+    L.status = mv::device_status_word(&rc);
+    if (rc) return rc;
+    L.jobs = jobs_dev;
+    L.njobs = njobs;
+    L.nitems = info->nitems;
+    L.batch = batch;
+    L.spin_limit = mv::wait_spin_limit();
+    L.drop_copy = mv::inject_drop_copy();
+    L.buf_words = (info->max_blk_rows + 1) * 32;
+    L.tbl_stage = (int)((info->tbl_stripe_max + 7) & ~7u);
+    L.lut_stride = 32;
+    L.chain_scales = chain_scales_dev;
+    L.chain_out8 = out8_dev;
+    mv::q8s_chain_reset<<<(njobs + 255) / 256, 256, 0, st>>>(reinterpret_cast<mv::Q8Job *>(jobs_dev), njobs);
+    MV_CUDA_TRY(cudaGetLastError(), "q8s_chain_reset launch");
+    return mv::launch_q8s(L, mv::nv_round(batch), t, st);
 }
 
 mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info, int batch,

@@ -269,6 +269,50 @@ class Q8Stack:
         return self.ys
 
 
+class Q8Chain:
+    """A chain of Q8 matrices run as the reference's end-to-end workload
+    (buffered/ans-warp-rows.cu:208-221): x_{j+1} = clamp(round(y_j * scale_j), -128, 127),
+    with y_j = W_j x_j, every step in ONE persistent, cooperative launch
+    (mv_q8_chain_matvec).  rows of matrix j must equal cols of matrix j+1.
+    After run(): xs[j] holds matrix j's input (xs[0] the given one), ys[j] its int32
+    output, out8 the final int8 vector(s) [batch, rows_last]."""
+
+    def __init__(self, matrices, scales, batch=1, tuning=None, x0=None, device="cuda"):
+        self.device = torch.device(device)
+        self.matrices = list(matrices)
+        self.batch = int(batch)
+        if not 1 <= self.batch <= 16:
+            raise ValueError("batch must be 1..16")
+        if len(scales) != len(self.matrices):
+            raise ValueError("one scale per matrix")
+        self.tuning = tuning if isinstance(tuning, Q8Tuning) else Q8Tuning(*(tuning or (0, 0, 0, 0)))
+        self.scales = torch.tensor([float(s) for s in scales], dtype=torch.float32, device=self.device)
+        self.xs = [x0 if x0 is not None else torch.zeros((self.batch, self.matrices[0].cols), dtype=torch.int8,
+                                                          device=self.device)]
+        self.xs += [torch.zeros((self.batch, M.cols), dtype=torch.int8, device=self.device)
+                    for M in self.matrices[1:]]
+        self.ys = [torch.empty((self.batch, M.rows), dtype=torch.int32, device=self.device) for M in self.matrices]
+        self.out8 = torch.empty((self.batch, self.matrices[-1].rows), dtype=torch.int8, device=self.device)
+        n = len(self.matrices)
+        jobs = (Q8Job * n)()
+        for i, M in enumerate(self.matrices):
+            x = self.xs[i]
+            if x.dtype != torch.int8 or tuple(x.shape) != (self.batch, M.cols) or not x.is_contiguous():
+                raise ValueError(f"x[{i}] must be a contiguous int8 tensor of shape {(self.batch, M.cols)}")
+            jobs[i].m = M.view()
+            jobs[i].x = x.data_ptr()
+            jobs[i].y = self.ys[i].data_ptr()
+        self.info = Q8StackInfo()
+        check(lib().mv_q8_chain_plan(jobs, n, ctypes.byref(self.tuning), ctypes.byref(self.info)))
+        raw = np.frombuffer(bytes(jobs), dtype=np.uint8)
+        self.jobs_dev = torch.from_numpy(raw.copy()).to(self.device)
+
+    def run(self):
+        check(lib().mv_q8_chain_matvec(_p(self.jobs_dev), len(self.matrices), ctypes.byref(self.info), self.batch,
+                                       _p(self.scales), _p(self.out8), ctypes.byref(self.tuning), _stream()))
+        return self.out8
+
+
 def dense_matvec(W, x, out=None):
     """Dense int8 comparator y = W x on the GPU (W [rows, cols] int8 device tensor)."""
     rows, cols = W.shape
