@@ -248,6 +248,46 @@ def build_stack(torch, ops, dev, layers=32, keep_dense=True):
     return mats
 
 
+def chain_section(torch, ops, autotune, dev, mats, batches=(1, 16), reps=5, scale=2e-3):
+    """The reference's chained workload over the stack's q,k,v,o,gate,down matrices (192, 4096 -> 4096 ->
+    ... -> 11008 -> 4096 per layer): x_{j+1} = clamp(rn(fp32(W_j x_j) * scale)).  Fused (one cooperative
+    launch), one chain launch per matrix, and the same matrices as an independent stack (no dependencies).
+    Gate: every step against the dense kernel and torch's fp32 round-half-even on the GPU."""
+    chain = [m for m in mats if not m["spec"]["name"].endswith(".up")]
+    Ms = [m["M"] for m in chain]
+    out = {"matrices": len(Ms)}
+    g = torch.Generator(device=dev)
+    g.manual_seed(123)
+    for B in batches:
+        x0 = torch.randint(-127, 128, (B, Ms[0].cols), dtype=torch.int8, device=dev, generator=g)
+        C = ops.Q8Chain(Ms, [scale] * len(Ms), batch=B, x0=x0, device=dev)
+        C.run()
+        torch.cuda.synchronize()
+        v = x0
+        for j, m in enumerate(chain):
+            y = ops.dense_matvec(m["Wd"], v)
+            v = torch.clamp(torch.round(y.float() * scale), -128, 127).to(torch.int8)
+            got = C.xs[j + 1] if j + 1 < len(Ms) else C.out8
+            if not torch.equal(got, v):
+                raise SystemExit(f"bench: chain step {j} (B={B}) is not bit-exact")
+        t_fused, gf = time_graph(torch, C.run, reps)
+        del gf
+        steps, xin = [], x0
+        for M in Ms:
+            c = ops.Q8Chain([M], [scale], batch=B, x0=xin, device=dev)
+            steps.append(c)
+            xin = c.out8
+        t_each, ge = time_graph(torch, lambda: [c.run() for c in steps], reps)
+        del ge
+        S = ops.Q8Stack(Ms, batch=B, device=dev)
+        t_stack, gs = time_graph(torch, S.run, reps)
+        del gs, S, steps
+        out[f"B{B}"] = {"fused_us": round(1e3 * t_fused, 1), "one_launch_per_matrix_us": round(1e3 * t_each, 1),
+                        "independent_stack_us": round(1e3 * t_stack, 1),
+                        "fused_speedup_vs_per_matrix": round(t_each / t_fused, 3)}
+    return out
+
+
 def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, reps=10):
     """configs: the 224-matrix uneven stack, one persistent launch per step, B in {1,4,8,16}; the tensor-core
     engine competes with dp4a at B >= 8.  Gate: bit-exact against the dense int8 kernel on the same x."""
@@ -312,6 +352,7 @@ def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, r
         row["speedup_vs_cublas_int8_gemm"] = None if t_gemm is None else round(1e3 * t_gemm / fastest["us_per_step"], 3)
         out["batches"][f"B{B}"] = row
         del xs, ref
+    out["chain192"] = chain_section(torch, ops, autotune, dev, mats, reps=reps)
     del mats, Ms
     torch.cuda.empty_cache()
     ops.device_status()

@@ -154,42 +154,28 @@ __device__ __forceinline__ void issue_step(const Q8SLaunch &L, const StepCursor 
     }
 }
 
-// x loads: through the read-only path, or (coh: x was written earlier in the same launch, by the
-// chained pipeline) through L2 only
-__device__ __forceinline__ uint4 ldx_u4(const void *p, bool coh) {
-    if (coh) {
-        uint4 v;
-        asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
-        return v;
-    }
-    return __ldg(reinterpret_cast<const uint4 *>(p));
-}
-__device__ __forceinline__ uint32_t ldx_u32(const void *p, bool coh) {
-    if (coh) {
-        uint32_t v;
-        asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(p));
-        return v;
-    }
-    return __ldg(reinterpret_cast<const uint32_t *>(p));
-}
+// x loads: plain (coherent, L1-cached) global loads rather than the read-only path.  In a chained
+// launch x was written earlier by other CTAs; the acquire load and CTA barrier of chain_wait order these
+// loads after those writes, which the read-only path would not guarantee.
+__device__ __forceinline__ uint4 ldx_u4(const void *p) { return *reinterpret_cast<const uint4 *>(p); }
+__device__ __forceinline__ uint32_t ldx_u32(const void *p) { return *reinterpret_cast<const uint32_t *>(p); }
 
 template <int NV>
-__device__ __forceinline__ void load_x(const int8_t *x, int cols, int q, uint32_t (&xv)[NV], bool coh) {
+__device__ __forceinline__ void load_x(const int8_t *x, int cols, int q, uint32_t (&xv)[NV]) {
 #pragma unroll
-    for (int v = 0; v < NV; v++) xv[v] = ldx_u32(reinterpret_cast<const uint32_t *>(x + (size_t)v * cols) + q, coh);
+    for (int v = 0; v < NV; v++) xv[v] = ldx_u32(reinterpret_cast<const uint32_t *>(x + (size_t)v * cols) + q);
 }
 
 // Four consecutive quads of x (16 bytes) per vector; q % 4 == 0.
 template <int NV>
-__device__ __forceinline__ void load_x4(const int8_t *x, int cols, int q, uint4 (&xv)[NV], bool coh) {
+__device__ __forceinline__ void load_x4(const int8_t *x, int cols, int q, uint4 (&xv)[NV]) {
 #pragma unroll
-    for (int v = 0; v < NV; v++) xv[v] = ldx_u4(x + (size_t)v * cols + 4 * q, coh);
+    for (int v = 0; v < NV; v++) xv[v] = ldx_u4(x + (size_t)v * cols + 4 * q);
 }
 
 // The chained pipeline's epilogue of one output: job j's int8 result, the reference's fp32
 // requantisation (ans-warp-rows-kernel.cu:212-220), stored as the next job's x.
-__device__ __forceinline__ void chain_emit(const Q8SLaunch &L, const Q8Job &J, int v, int row, int sum) {
-    const int j = (int)(&J - L.jobs);
+__device__ __forceinline__ void chain_emit(const Q8SLaunch &L, const Q8Job &J, int j, int v, int row, int sum) {
     const int r = __float2int_rn((float)sum * __ldg(L.chain_scales + j));
     int8_t *o = j + 1 < L.njobs ? const_cast<int8_t *>(L.jobs[j + 1].x) : L.chain_out8;
     o[(size_t)v * J.m.rows + row] = (int8_t)max(-128, min(127, r));
@@ -245,6 +231,7 @@ struct IntCons {
     static constexpr int kNV = NV;
     static constexpr int kRedNV = NV;
     static constexpr int kMinCtas = 1;
+    static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
@@ -255,24 +242,23 @@ struct IntCons {
                                              const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
                                              int lane);
     const int8_t *x;
-    int cols;
-    bool coh;
+    int cols, job_idx;
     int acc[NV];
     struct Group {
         uint4 xv[NV];
     };
-    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int, int job) {
         x = J.x;
         cols = J.m.cols;
-        coh = L.chain_scales != nullptr;
+        job_idx = job;
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = 0;
     }
-    __device__ __forceinline__ void load_group(Group &g, int q) const { load_x4<NV>(x, cols, q, g.xv, coh); }
+    __device__ __forceinline__ void load_group(Group &g, int q) const { load_x4<NV>(x, cols, q, g.xv); }
     __device__ __forceinline__ void use(const Group &g, int j, int, uint32_t wq, int) { dot4<NV>(wq, g.xv, j, acc); }
     __device__ __forceinline__ void single(int q, uint32_t wq, int) {
         uint32_t xv[NV];
-        load_x<NV>(x, cols, q, xv, coh);
+        load_x<NV>(x, cols, q, xv);
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wq, (int)xv[v], acc[v]);
     }
@@ -295,7 +281,7 @@ struct IntCons {
                 } else {
                     *dst = sum;
                     if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
-                    if (L.chain_scales) chain_emit(L, J, v, row, sum);
+                    if (L.chain_scales) chain_emit(L, J, job_idx, v, row, sum);
                 }
             }
         }
@@ -322,6 +308,7 @@ struct FwdCons {
     static constexpr int kNV = NV;
     static constexpr int kRedNV = NV;
     static constexpr int kMinCtas = 1;
+    static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
@@ -337,7 +324,7 @@ struct FwdCons {
     struct Group {
         uint4 xv[NV][2];  // 16 bf16 = 4 quads
     };
-    __device__ __forceinline__ void begin_item(const Q8SLaunch &, const Q8Job &J, int, int) {
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &, const Q8Job &J, int, int, int) {
         x = reinterpret_cast<const uint16_t *>(J.x);
         cols = J.m.cols;
 #pragma unroll
@@ -407,6 +394,7 @@ struct BwdCons {
     static constexpr int kNV = NV;
     static constexpr int kRedNV = NV;
     static constexpr int kMinCtas = 1;
+    static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
@@ -420,7 +408,7 @@ struct BwdCons {
     float *dx;
     int cols;
     struct Group {};
-    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int lane) {
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int lane, int) {
         const int row = stripe * 32 + lane;
         const uint16_t *dy = reinterpret_cast<const uint16_t *>(J.x);
         dx = J.ys;
@@ -567,7 +555,8 @@ __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const 
 struct MmaCons {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;      // reduction area: the x tiles
-    static constexpr int kMinCtas = 2;    // 2 x 8 warps per SM: at most 128 registers per thread
+    static constexpr int kMinCtas = 1;    // with up to 16 warps: at most 128 registers per thread
+    static constexpr int kMaxThreads = 512;  // 1 x 16 or 2 x 8 warps per SM
     static constexpr int kTmemCols = 1;   // > 0: the kernel allocates TMEM
     static constexpr int kXChunks = 4;    // x tile: 4 pieces of 32 columns x 16 vectors (512 B each)
     static constexpr int kXBytes = kXChunks * 512;
@@ -586,8 +575,8 @@ struct MmaCons {
     uint64_t *mbar;
     int *xbase;
     const int8_t *x;
-    int cols, batch;
-    bool any, coh;
+    int cols, batch, job_idx;
+    bool any;
 
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int,
                                          int lane, int W) {
@@ -610,12 +599,12 @@ struct MmaCons {
         b_desc0 = umma_smem_desc(xt, 128u, 256u);
         ncommit = 0;
     }
-    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int, int job) {
         x = J.x;
         cols = J.m.cols;
         batch = L.batch;
         any = false;
-        coh = L.chain_scales != nullptr;
+        job_idx = job;
     }
     // wait until every MMA issued so far completed (the latest commit covers all earlier MMAs)
     __device__ __forceinline__ bool wait_mma(const Q8SLaunch &L) {
@@ -645,7 +634,7 @@ struct MmaCons {
             const int c = pbase + i;
             xr[i] = make_uint4(0, 0, 0, 0);
             // cols % 16 == 0, so a 16-byte piece that starts inside the row ends inside it
-            if (xok && c < npieces && colbase + 32 * c < cols) xr[i] = ldx_u4(xrow + 32 * c, coh);
+            if (xok && c < npieces && colbase + 32 * c < cols) xr[i] = ldx_u4(xrow + 32 * c);
         }
     }
     template <int ILP>
@@ -742,7 +731,7 @@ struct MmaCons {
                 } else {
                     *dst = sum;
                     if (J.ys) J.ys[(size_t)v * m.rows + row] = (float)sum * J.scales[row];
-                    if (L.chain_scales) chain_emit(L, J, v, row, sum);
+                    if (L.chain_scales) chain_emit(L, J, job_idx, v, row, sum);
                 }
             }
         }
@@ -786,6 +775,7 @@ struct FwdMma {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;
     static constexpr int kMinCtas = 2;
+    static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
     static constexpr int kXPieces = 2;
     static constexpr int kXBytes = kXPieces * 1024;
@@ -818,7 +808,7 @@ struct FwdMma {
         b_desc0 = umma_smem_desc(xt, 128u, 256u);
         ncommit = 0;
     }
-    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int) {
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int, int) {
         x = reinterpret_cast<const uint16_t *>(J.x);
         cols = J.m.cols;
         batch = L.batch;
@@ -957,6 +947,7 @@ struct BwdMma {
     static constexpr int kNV = 32;
     static constexpr int kRedNV = 0;
     static constexpr int kMinCtas = 2;
+    static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
     static constexpr int kGBytes = 4096;  // [hi, lo][K step 0, 1] x 1 KB
     static constexpr int kWBytes = 2048;  // W tile per warp: 2 K steps x 1 KB
@@ -995,7 +986,7 @@ struct BwdMma {
         return mbar_wait_bounded(mbar, (ncommit - 1) & 1, L.status, L.spin_limit);
     }
     // CTA-wide (every warp calls it for the same item): G = s . dY of the stripe as bf16 hi/lo tiles
-    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int) {
+    __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int, int) {
         const uint16_t *dy = reinterpret_cast<const uint16_t *>(J.x);
         dx = J.ys;
         cols = J.m.cols;
@@ -1119,7 +1110,7 @@ __global__ void q8s_chain_reset(Q8Job *jobs, int njobs) {
 }
 
 template <class Cons, int ILP, int DEPTH>
-__global__ void __launch_bounds__(256, Cons::kMinCtas) q8s_kernel(const Q8SLaunch L) {
+__global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(const Q8SLaunch L) {
     constexpr int NV = Cons::kRedNV;
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1219,7 +1210,7 @@ __global__ void __launch_bounds__(256, Cons::kMinCtas) q8s_kernel(const Q8SLaunc
         }
 
         if (L.chain_scales && I.job > 0) chain_wait(L, I.job - 1);
-        cons.begin_item(L, J, I.stripe, lane);
+        cons.begin_item(L, J, I.stripe, lane, I.job);
         const int steps = warp_steps(send - sbeg, warp, W, ILP);
         for (int j = 0; j < steps; j++) {
             const int slot = consumed % DEPTH;
@@ -1314,6 +1305,9 @@ mv_status resident_ctas(const void *kern, size_t smem, int threads, int *out) {
 
 template <class Cons, int ILP, int DEPTH>
 mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t st) {
+    if (32 * W > Cons::kMaxThreads)
+        return fail(MV_ERR_ARG, "Q8 launch: %d warps per CTA; this engine takes at most %d", W,
+                    Cons::kMaxThreads / 32);
     if (Cons::extra_bytes(W) % 16)  // the stream buffers behind the consumer region take bulk copies
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch: consumer region of %zu B breaks 16-byte alignment",
                     Cons::extra_bytes(W));
@@ -1336,7 +1330,12 @@ mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t 
         bps = std::max(1, std::min<int>(bps, 512 / MmaCons::tmem_cols(W)));
     }
     if (L.chain_scales) {
-        // the chained pipeline waits across CTAs: a cooperative launch guarantees that they are all resident
+        // the chained pipeline waits across CTAs: a cooperative launch guarantees that they are all resident.
+        // The runtime checks the grid against its own occupancy figure, which for tensor-memory kernels is
+        // lower than what the SM holds; a grid it rejects as too large is retried at that figure.
+        // The runtime checks the grid against its own occupancy figure (for tensor-memory kernels one CTA
+        // per SM, fewer than the SM holds), and a rejected launch would also end a stream capture, so the
+        // grid is taken from that figure; 16-warp CTAs keep a tensor-core chain at 16 warps per SM.
         int coop = 0;
         MV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&coop, kern, 32 * W, smem), "occupancy");
         coop = std::max(1, std::min(coop, bps));
@@ -1414,7 +1413,7 @@ mv_q8_tuning resolve(const mv_q8_tuning *t) {
     if (t) {
         if (t->engine == MV_ENGINE_DP4A) r.engine = MV_ENGINE_DP4A;
         if (t->parts > 0) r.parts = t->parts;
-        if (t->warps > 0) r.warps = std::min(8, t->warps);
+        if (t->warps > 0) r.warps = std::min(16, t->warps);  // more than 8: tensor-core engine only
         if (t->ilp == 1 || t->ilp == 2) r.ilp = t->ilp;
         if (t->depth == 1 || t->depth == 2) r.depth = t->depth;
         if (t->ctas_per_sm > 0) r.ctas_per_sm = t->ctas_per_sm;

@@ -66,9 +66,9 @@ def test_chain_reproduces_reference_hashes(local):
 
 
 @pytest.mark.parametrize("B", [1, 3, 8, 16])
-@pytest.mark.parametrize("tuning", [(4, 1, 1, 0), (8, 2, 2, 0), (1, 1, 1, 0), (8, 1, 1, 0, 0, 1)])
+@pytest.mark.parametrize("tuning", [(4, 1, 1, 0), (8, 2, 2, 0), (1, 1, 1, 0), (8, 1, 1, 0, 0, 1), None])
 def test_chain_random(B, tuning):
-    rng = np.random.default_rng(B * 7 + tuning[0])
+    rng = np.random.default_rng(B * 7 + (tuning or (0,))[0])
     dims = [512, 1008, 256, 4096, 512]
     Ws = [gauss(rng, rng.uniform(2, 6), (dims[i + 1], dims[i])) for i in range(len(dims) - 1)]
     Ms = [ops.Q8Matrix.encode(W, local=(i % 2 == 0)) for i, W in enumerate(Ws)]
