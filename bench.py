@@ -556,7 +556,7 @@ def run_ours(args):
                           "entropy_bits": e["entropy"],
                           "tuning": [tun.warps, tun.ilp, tun.depth, tun.ctas_per_sm, tun.parts]}
     torch.cuda.empty_cache()
-    dense, cublas, awr_t, wpr_t = {}, {}, {}, {}
+    dense, cublas, awr_t, wpr_t, aws_t = {}, {}, {}, {}, {}
     for m in mats:
         if m["sigma"] != 4.0:
             continue
@@ -585,6 +585,14 @@ def run_ours(args):
         t_ms, _ = time_graph(torch, lambda: [a.matvec(x1, out=yd) for a in As], 10, inner=R)
         awr_t[key] = {"us": 1e3 * t_ms, "bits_per_weight": 32.0 * A.n_words / (rows * cols)}
         del As, A
+        S_ = ops.AwsMatrix.encode(m["W"], device=dev)
+        R = copies_for(4 * S_.n_words)
+        Ss = [S_] + [ops.AwsMatrix(S_.compressed.cpu().numpy(), S_.offsets.cpu().numpy(), S_.ppf.cpu().numpy(),
+                                   S_.ppf_cum.cpu().numpy(), S_.ppf_prob.cpu().numpy(), rows, cols, dev)
+                     for _ in range(R - 1)]
+        t_ms, _ = time_graph(torch, lambda: [a.matvec(x1, out=yd) for a in Ss], 10, inner=R)
+        aws_t[key] = {"us": 1e3 * t_ms, "bits_per_weight": 32.0 * S_.n_words / (rows * cols)}
+        del Ss, S_
         if cols % 512 == 0 and rows == cols:
             P = ops.WprMatrix.encode(m["W"], device=dev)
             R = copies_for(2 * P.payload_size)
@@ -668,6 +676,7 @@ def run_ours(args):
             "per_matrix": per,
             "dense_dp4a": dense, "cublas_sgemv_fp32": cublas, "ans_warp_rows_kernel": awr_t,
             "warp_per_row_kernel": wpr_t,
+            "ans_warp_stripes_kernel": aws_t,
             "float_form": float_form,
             "stack224": stack224,
             "large_low_entropy": large,

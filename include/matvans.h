@@ -98,6 +98,36 @@ mv_status mv_awr_matvec_requant(const uint32_t *compressed_dev, size_t n_words,
                                 int rows, int cols, const int8_t *x_dev, float scale,
                                 int8_t *out8_dev, void *stream);
 
+/* ------------------------------------------------------------- stripes --- */
+
+/* The reference's "ans-warp-stripes" layout (buffered/encoder.py:323-391,
+ * kernel ans-warp-stripes-kernel.cu:21-227): the AWR coder and word stream,
+ * but a warp decodes a stripe of 32 rows, lane l row 32s+l, one quad per lane
+ * per step; warp_offsets has one entry per stripe (uint4 units).  Exact int32
+ * y for `batch` vectors.  rows % 32 == 0, cols % 4 == 0. */
+mv_status mv_aws_matvec(const uint32_t *compressed_dev, size_t n_words,
+                        const uint32_t *warp_offsets_dev, const uint32_t *ppf_dev,
+                        const uint32_t *ppf_cum_dev, const uint32_t *ppf_prob_dev, int rows,
+                        int cols, const int8_t *x_dev, int batch, int32_t *y_dev,
+                        const float *row_scales_dev, float *y_scaled_dev, void *stream);
+
+/* Fused decode + dot product + requantisation, the reference kernel's output:
+ * out8[r] = clamp(round_half_even((float)y[r] * scale), -128, 127). */
+mv_status mv_aws_matvec_requant(const uint32_t *compressed_dev, size_t n_words,
+                                const uint32_t *warp_offsets_dev, const uint32_t *ppf_dev,
+                                const uint32_t *ppf_cum_dev, const uint32_t *ppf_prob_dev,
+                                int rows, int cols, const int8_t *x_dev, float scale,
+                                int8_t *out8_dev, void *stream);
+
+/* Replaces the launcher of buffered/ans-warp-stripes.cu:38-60, which has the
+ * same name and arguments as the rows program's mat_vec_mul_coalesced; renamed
+ * so that both layouts live in one library.  Legacy default stream; errors go
+ * to stderr and mv_last_error(). */
+void mat_vec_mul_coalesced_stripes(const void *in_vector_gpu, void *out_vector_gpu, size_t in_dim,
+                                   size_t out_dim, float scale, const void *compressed,
+                                   const uint32_t *warp_offsets, const uint32_t *ppf,
+                                   const uint32_t *ppf_cum, const uint32_t *ppf_prob);
+
 /* ------------------------------------------------------------------ WPR --- */
 
 /* Replaces the kernel launch in CompressedMatrix::decompressAndMult,
@@ -297,6 +327,12 @@ const char *mv_blob_name(const mv_blob *b, int i);
  * Fails with MV_ERR_SHAPE unless cols % 128 == 0, and MV_ERR_UNSUPPORTED for
  * more than 128 distinct values (encoder.py:303). */
 mv_status mv_awr_encode(const int8_t *W, int rows, int cols, int nthreads, mv_blob **out);
+
+/* Reference-compatible "ans-warp-stripes" encoder: byte-identical to
+ * compress_ans_warp_stripes(W, 32) of buffered/encoder.py:323-391 (same model
+ * and tables as mv_awr_encode).  Arrays as mv_awr_encode, with
+ * "warp_offsets" u32[rows/32].  rows % 32 == 0, cols % 4 == 0. */
+mv_status mv_aws_encode(const int8_t *W, int rows, int cols, int nthreads, mv_blob **out);
 
 /* Reference-compatible WPR encoder: encode_matrix of
  * create_matrices_WarpPerRow.py:353-430 with create_entropy_model (:131-187)

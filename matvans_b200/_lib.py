@@ -25,6 +25,7 @@ EXPORTS = [
     "mv_wpr_encode", "mv_q8_encode", "mv_read_safetensors", "mv_write_safetensors", "mv_read_wpr_bin",
     "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc", "mv_q8_matvec_tuned", "mv_q8_stack_plan",
     "mv_q8_stack_matvec", "mv_q8_matvec_bf16", "mv_q8_matvec_t_bf16", "mv_q8_chain_plan", "mv_q8_chain_matvec",
+    "mv_aws_matvec", "mv_aws_matvec_requant", "mv_aws_encode", "mat_vec_mul_coalesced_stripes",
 ]
 
 
@@ -81,6 +82,9 @@ def lib():
         "mat_vec_mul_coalesced": ([P, P, sz, sz, ctypes.c_float, P, P, P, P, P], None),
         "mv_awr_matvec": ([P, sz, P, P, P, P, i32, i32, P, i32, P, P, P, P], st),
         "mv_awr_matvec_requant": ([P, sz, P, P, P, P, i32, i32, P, ctypes.c_float, P, P], st),
+        "mat_vec_mul_coalesced_stripes": ([P, P, sz, sz, ctypes.c_float, P, P, P, P, P], None),
+        "mv_aws_matvec": ([P, sz, P, P, P, P, i32, i32, P, i32, P, P, P, P], st),
+        "mv_aws_matvec_requant": ([P, sz, P, P, P, P, i32, i32, P, ctypes.c_float, P, P], st),
         "mv_wpr_matvec": ([P, sz, P, ctypes.c_int8, P, i32, P, i32, i32, P, i32, P, P, P, P], st),
         "mv_requant_absmax": ([P, i32, P, P, P, P], st),
         "mv_requant_absmax_noalloc": ([P, i32, P, P, P], st),
@@ -99,6 +103,7 @@ def lib():
         "mv_blob_get_i64": ([P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)], st),
         "mv_blob_name": ([P, i32], ctypes.c_char_p),
         "mv_awr_encode": ([P, i32, i32, i32, ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_aws_encode": ([P, i32, i32, i32, ctypes.POINTER(ctypes.c_void_p)], st),
         "mv_wpr_encode": ([P, i32, i32, i32, ctypes.POINTER(ctypes.c_void_p)], st),
         "mv_q8_encode": ([P, i32, i32, i32, i32, i32, ctypes.POINTER(ctypes.c_void_p)], st),
         "mv_read_safetensors": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)], st),

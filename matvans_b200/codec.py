@@ -65,6 +65,21 @@ def compress_ans_warp_rows(matrix, warp_size=32):
             b.array("cdf", np.uint8))
 
 
+def compress_ans_warp_stripes(matrix, warp_size=32):
+    """Returns (compressed u32, warp_offsets u32 [rows/32] in uint4 units, min_value, cdf u8),
+    byte-identical to buffered/encoder.py:323-391 (rows % 32 == 0, cols % 4 == 0)."""
+    if warp_size != 32:
+        raise ValueError("the ans-warp-stripes layout is defined for warp_size 32")
+    W = _i8(matrix)
+    if W.ndim != 2:
+        raise ValueError("matrix must have rank 2")
+    h = _lib.new_blob_out()
+    check(lib().mv_aws_encode(ptr(W), W.shape[0], W.shape[1], 0, ctypes.byref(h)))
+    b = Blob(h.value)
+    return (b.array("compressed", np.uint32), b.array("warp_offsets", np.uint32), b.scalar("min_value"),
+            b.array("cdf", np.uint8))
+
+
 def fit_128bit_encoder_model(data):
     """(entropy, cross_entropy, min_value, cdf) as buffered/encoder.py:271-306.
 
@@ -117,14 +132,14 @@ def pack_4bytes(arr):
 
 
 def compress_all_matrices(matrices, initial_vector, scales, hashes, compressor, filename):
-    """Writes the safetensors file of buffered/encoder.py:473-511 (compressor must be
-    compress_ans_warp_rows; the stripes layout is not part of this library)."""
-    if compressor is not compress_ans_warp_rows:
-        raise ValueError("only compress_ans_warp_rows is supported")
+    """Writes the safetensors file of buffered/encoder.py:473-511 (compressor:
+    compress_ans_warp_rows or compress_ans_warp_stripes)."""
+    if compressor not in (compress_ans_warp_rows, compress_ans_warp_stripes):
+        raise ValueError("compressor must be compress_ans_warp_rows or compress_ans_warp_stripes")
     comp, offs, ppfs, cums, probs = [], [], [], [], []
     size = 0
     for m in matrices:
-        c, o, mn, cdf = compress_ans_warp_rows(m, 32)
+        c, o, mn, cdf = compressor(m, 32)
         p, pc, pp = decoder_model_from_128bit_encoder_model(mn, cdf)
         comp.append(c)
         offs.append(o + size)

@@ -6,6 +6,7 @@
 //                           :271-306 (fit_128bit_encoder_model),
 //                           :309-320 (decoder_model_from_128bit_encoder_model),
 //                           :394-461 (compress_ans_warp_rows), :464-470 (pack_4bytes)
+//   AWS ("ans-warp-stripes"): the same coder and model, :323-391 (compress_ans_warp_stripes)
 //   WPR ("matvansWarpPerRow"): matvansWarpPerRow/create_matrices_WarpPerRow.py:
 //                           :131-187 (create_entropy_model), :189-208 (create_ppf),
 //                           :211-272 (AnsCoder), :353-430 (encode_matrix)
@@ -125,7 +126,76 @@ inline void awr_encode_quad(uint64_t &state, const int8_t *quad, const AwrModel 
     state = (state << 28) | concat;
 }
 
+// The word stream of one warp (an AWR row or an "ans-warp-stripes" stripe) as the decoder reads it
+// (encoder.py:431-447 and :355-383, identical steps): the joint bulk of the 32 coders reversed, padded
+// with zeros to a length of 64 (mod 128), the 32 low then the 32 high state words inserted at word 64,
+// and every 128-word block transposed so that lane l's uint4 holds words (l, 32+l, 64+l, 96+l).
+void awr_assemble(const std::vector<uint32_t> &buf, const uint64_t (&state)[32], std::vector<uint32_t> &bulk,
+                  std::vector<uint32_t> &compressed) {
+    bulk.assign(buf.rbegin(), buf.rend());
+    int64_t pad = ((64 - (int64_t)bulk.size()) % 128 + 128) % 128;
+    bulk.resize(bulk.size() + pad, 0u);
+    std::vector<uint32_t> un;
+    un.reserve(bulk.size() + 64);
+    un.insert(un.end(), bulk.begin(), bulk.begin() + 64);
+    for (int l = 0; l < 32; l++) un.push_back((uint32_t)state[l]);
+    for (int l = 0; l < 32; l++) un.push_back((uint32_t)(state[l] >> 32));
+    un.insert(un.end(), bulk.begin() + 64, bulk.end());
+    const size_t blocks = un.size() / 128;
+    for (size_t b = 0; b < blocks; b++)
+        for (int l = 0; l < 32; l++)
+            for (int f = 0; f < 4; f++) compressed.push_back(un[b * 128 + f * 32 + l]);
+}
+
+void awr_put_tables(const AwrModel &m, Blob &out) {
+    uint32_t ppf[32], cum[32], prob[32];
+    awr_decoder_tables(m, ppf, cum, prob);
+    out.put("cdf", m.cdf);
+    out.shape("cdf", DT_U8, {(int64_t)m.cdf.size()});
+    out.put("ppf", std::vector<uint32_t>(ppf, ppf + 32));
+    out.put("ppf_cum", std::vector<uint32_t>(cum, cum + 32));
+    out.put("ppf_prob", std::vector<uint32_t>(prob, prob + 32));
+    for (const char *n : {"ppf", "ppf_cum", "ppf_prob"}) out.shape(n, DT_U32, {32});
+    out.set("min_value", m.min_value);
+}
+
 }  // namespace
+
+// compress_ans_warp_stripes(matrix, 32), encoder.py:323-391.  Lane l of stripe s is row 32s + l; a
+// stripe's quads are coded column by column from the last (lanes 31..0 within a column) into one joint
+// stream, and, as in the rows layout, the 32 coders carry their states from stripe to stripe.
+static mv_status aws_encode(const int8_t *W, int rows, int cols, Blob &out) {
+    if (!W || rows <= 0 || cols <= 0) return fail(MV_ERR_ARG, "mv_aws_encode: bad arguments");
+    if (rows % 32 || cols % 4)
+        return fail(MV_ERR_SHAPE, "stripes layout needs rows %% 32 == 0 and cols %% 4 == 0 (%dx%d)", rows, cols);
+    AwrModel m;
+    mv_status st = fit_awr_model(W, (int64_t)rows * cols, m);
+    if (st) return st;
+    for (int64_t i = 0; i < (int64_t)rows * cols; i++) {
+        int idx = W[i] - m.min_value;
+        if (m.cdf[idx + 1] == m.cdf[idx]) return fail(MV_ERR_FORMAT, "AWR model lost a symbol");
+    }
+    const int stripes = rows / 32, quads = cols / 4;
+    std::vector<uint32_t> compressed, offsets(stripes), buf, bulk;
+    uint64_t state[32] = {0};
+    for (int s = 0; s < stripes; s++) {
+        if (compressed.size() / 4 > 0xFFFFFFFFull) return fail(MV_ERR_SHAPE, "stripes offsets overflow 32 bits");
+        offsets[s] = (uint32_t)(compressed.size() / 4);
+        buf.clear();
+        for (int c = quads - 1; c >= 0; c--)
+            for (int l = 31; l >= 0; l--)
+                awr_encode_quad(state[l], W + ((int64_t)s * 32 + l) * cols + 4 * c, m, buf);
+        awr_assemble(buf, state, bulk, compressed);
+    }
+    out.put("compressed", compressed);
+    out.shape("compressed", DT_U32, {(int64_t)compressed.size()});
+    out.put("warp_offsets", offsets);
+    out.shape("warp_offsets", DT_U32, {stripes});
+    awr_put_tables(m, out);
+    out.set("rows", rows);
+    out.set("cols", cols);
+    return MV_OK;
+}
 
 // compress_ans_warp_rows(matrix, 32), encoder.py:394-461.  The 32 coders are
 // created once per matrix and are NOT reset between rows (encoder.py:402), so
@@ -154,34 +224,13 @@ static mv_status awr_encode(const int8_t *W, int rows, int cols, Blob &out) {
         const int8_t *row = W + (int64_t)r * cols;
         for (int c = chunks - 1; c >= 0; c--)
             for (int l = 31; l >= 0; l--) awr_encode_quad(state[l], row + 128 * c + 4 * l, m, buf);
-        // reverse, pad to len = 64 (mod 128), insert states at 64, transpose (encoder.py:431-447)
-        bulk.assign(buf.rbegin(), buf.rend());
-        int64_t pad = ((64 - (int64_t)bulk.size()) % 128 + 128) % 128;
-        bulk.resize(bulk.size() + pad, 0u);
-        std::vector<uint32_t> un;
-        un.reserve(bulk.size() + 64);
-        un.insert(un.end(), bulk.begin(), bulk.begin() + 64);
-        for (int l = 0; l < 32; l++) un.push_back((uint32_t)state[l]);
-        for (int l = 0; l < 32; l++) un.push_back((uint32_t)(state[l] >> 32));
-        un.insert(un.end(), bulk.begin() + 64, bulk.end());
-        const size_t blocks = un.size() / 128;
-        for (size_t b = 0; b < blocks; b++)
-            for (int l = 0; l < 32; l++)
-                for (int f = 0; f < 4; f++) compressed.push_back(un[b * 128 + f * 32 + l]);
+        awr_assemble(buf, state, bulk, compressed);
     }
-    uint32_t ppf[32], cum[32], prob[32];
-    awr_decoder_tables(m, ppf, cum, prob);
     out.put("compressed", compressed);
     out.shape("compressed", DT_U32, {(int64_t)compressed.size()});
     out.put("warp_offsets", offsets);
     out.shape("warp_offsets", DT_U32, {rows});
-    out.put("cdf", m.cdf);
-    out.shape("cdf", DT_U8, {(int64_t)m.cdf.size()});
-    out.put("ppf", std::vector<uint32_t>(ppf, ppf + 32));
-    out.put("ppf_cum", std::vector<uint32_t>(cum, cum + 32));
-    out.put("ppf_prob", std::vector<uint32_t>(prob, prob + 32));
-    for (const char *n : {"ppf", "ppf_cum", "ppf_prob"}) out.shape(n, DT_U32, {32});
-    out.set("min_value", m.min_value);
+    awr_put_tables(m, out);
     out.set("rows", rows);
     out.set("cols", cols);
     return MV_OK;
@@ -353,6 +402,17 @@ mv_status mv_awr_encode(const int8_t *W, int rows, int cols, int nthreads, mv_bl
     auto *b = new (std::nothrow) mv_blob;
     if (!b) return mv::fail(MV_ERR_NOMEM, "mv_awr_encode: out of memory");
     mv_status st = mv::awr_encode(W, rows, cols, *b);
+    if (st) { delete b; return st; }
+    *out = b;
+    return MV_OK;
+}
+
+mv_status mv_aws_encode(const int8_t *W, int rows, int cols, int nthreads, mv_blob **out) {
+    (void)nthreads;  // stripes depend on each other (shared coders); encoded in order
+    if (!out) return mv::fail(MV_ERR_ARG, "mv_aws_encode: NULL out");
+    auto *b = new (std::nothrow) mv_blob;
+    if (!b) return mv::fail(MV_ERR_NOMEM, "mv_aws_encode: out of memory");
+    mv_status st = mv::aws_encode(W, rows, cols, *b);
     if (st) { delete b; return st; }
     *out = b;
     return MV_OK;

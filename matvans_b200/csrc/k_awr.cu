@@ -41,7 +41,11 @@ struct AwrLaunch {
     uint32_t *status;
 };
 
-template <int NV, bool REQUANT>
+// STRIPES: the "ans-warp-stripes" layout (ans-warp-stripes-kernel.cu:21-227, encoder.py:323-391).  The
+// word stream and its cache are the same, but a warp is a stripe of 32 rows: lane l is row 32u + l,
+// decodes its quad j (columns 4j..4j+3) at step j and keeps its own sums (no warp reduction), and
+// there is one offset per stripe.
+template <int NV, bool REQUANT, bool STRIPES>
 __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t *lut = reinterpret_cast<uint32_t *>(smem);  // 128 * 32 words
@@ -74,7 +78,8 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
     const uint32_t *lut_l = lut + lane;
     const bool bounded = L.n_u4 != 0;
 
-    for (int row = blockIdx.x * W + warp; row < L.rows; row += gridDim.x * W) {
+    const int units = STRIPES ? L.rows / 32 : L.rows;  // warps' work units: rows or 32-row stripes
+    for (int row = blockIdx.x * W + warp; row < units; row += gridDim.x * W) {
         size_t bi = __ldg(L.offs + row);  // uint4 index of the block held in `cache`
         uint4 cache = make_uint4(0, 0, 0, 0), nxt = make_uint4(0, 0, 0, 0);
         bool ovf = false;
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = 0;
 
-        for (int j = 0; j < nq; j += 32) {
+        for (int j = 0; j < nq; j += STRIPES ? 1 : 32) {
             const bool need = (state >> 32) == 0;
             const uint32_t ballot = __ballot_sync(0xffffffffu, need);
             if (ballot) {
@@ -141,11 +146,26 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
             state = (state >> 28) * (unsigned long long)p0123 + ns;
             const uint32_t wq =
                 __byte_perm(__byte_perm(e0, e1, 0x0040), __byte_perm(e2, e3, 0x0040), 0x5410);
-            const uint32_t *xq = xs + (j + lane) * NV;
+            const uint32_t *xq = xs + (STRIPES ? j : j + lane) * NV;  // stripes: one x quad for all lanes
 #pragma unroll
             for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wq, (int)xq[v], acc[v]);
         }
         if (ovf) atomicOr(L.status, MV_DEV_STREAM_OVERRUN);
+        if (STRIPES) {
+            const int r = row * 32 + lane;  // rows % 32 == 0
+            if (REQUANT) {
+                const int q = __float2int_rn((float)acc[0] * L.scale);  // ans-warp-stripes-kernel.cu:220-225
+                L.out8[r] = (int8_t)max(-128, min(127, q));
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; v++)
+                    if (v < L.batch) {
+                        L.y[(size_t)v * L.rows + r] = acc[v];
+                        if (L.ys) L.ys[(size_t)v * L.rows + r] = (float)acc[v] * L.scales[r];
+                    }
+            }
+            continue;
+        }
 #pragma unroll
         for (int v = 0; v < NV; v++) {
 #pragma unroll
@@ -170,17 +190,20 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
 
 namespace {
 
-template <int NV, bool REQUANT>
+template <int NV, bool REQUANT, bool STRIPES = false>
 mv_status launch_awr(const AwrLaunch &L, cudaStream_t st) {
-    const int W = 8;
+    // stripes: few work units (rows / 32, each decoded start to end by one warp), so one-warp CTAs spread
+    // them over all SMs
+    const int W = STRIPES ? 1 : 8;
     const size_t smem = 128 * 32 * 4 + (size_t)(L.cols / 4) * NV * 4;
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "AWR: %d columns x %d vectors exceed shared memory", L.cols, NV);
-    auto kern = awr_kernel<NV, REQUANT>;
+    auto kern = awr_kernel<NV, REQUANT, STRIPES>;
     int blocks_per_sm = 0;
     mv_status rc = prepare_kernel((const void *)kern, smem, 32 * W, &blocks_per_sm);
     if (rc) return rc;
-    const int want = (L.rows + W - 1) / W;
+    const int units = STRIPES ? L.rows / 32 : L.rows;
+    const int want = (units + W - 1) / W;
     const int grid = std::max(1, std::min(want, std::max(1, blocks_per_sm) * sm_count()));
     kern<<<grid, 32 * W, smem, st>>>(L);
     MV_CUDA_TRY(cudaGetLastError(), "awr kernel launch");
@@ -189,10 +212,15 @@ mv_status launch_awr(const AwrLaunch &L, cudaStream_t st) {
 
 mv_status awr_common(const uint32_t *comp, size_t n_words, const uint32_t *offs, const uint32_t *ppf,
                      const uint32_t *cum, const uint32_t *prob, int rows, int cols, const int8_t *x,
-                     AwrLaunch &L) {
+                     AwrLaunch &L, bool stripes = false) {
     if (!comp || !offs || !ppf || !cum || !prob || !x) return fail(MV_ERR_ARG, "mv_awr: NULL pointer");
     if (rows <= 0 || cols <= 0) return fail(MV_ERR_ARG, "mv_awr: rows/cols must be positive");
-    if (cols % 128) return fail(MV_ERR_SHAPE, "AWR layout needs cols %% 128 == 0 (cols=%d)", cols);
+    if (stripes) {
+        if (rows % 32 || cols % 4)
+            return fail(MV_ERR_SHAPE, "stripes layout needs rows %% 32 == 0 and cols %% 4 == 0 (%dx%d)", rows, cols);
+    } else if (cols % 128) {
+        return fail(MV_ERR_SHAPE, "AWR layout needs cols %% 128 == 0 (cols=%d)", cols);
+    }
     if (((uintptr_t)comp & 15) != 0) return fail(MV_ERR_ARG, "mv_awr: compressed not 16-byte aligned");
     mv_status rc;
     L.status = device_status_word(&rc);
@@ -236,6 +264,46 @@ mv_status awr_matvec(const uint32_t *comp, size_t n_words, const uint32_t *offs,
         if (rc) return rc;
     }
     return MV_OK;
+}
+
+mv_status aws_matvec(const uint32_t *comp, size_t n_words, const uint32_t *offs, const uint32_t *ppf,
+                     const uint32_t *cum, const uint32_t *prob, int rows, int cols, const int8_t *x,
+                     int batch, int32_t *y, const float *scales, float *ys, cudaStream_t st) {
+    AwrLaunch L{};
+    mv_status rc = awr_common(comp, n_words, offs, ppf, cum, prob, rows, cols, x, L, true);
+    if (rc) return rc;
+    if (!y || batch <= 0) return fail(MV_ERR_ARG, "mv_aws_matvec: bad y/batch");
+    if (n_words == 0) return fail(MV_ERR_ARG, "mv_aws_matvec: n_words must be given");
+    if (ys && !scales) return fail(MV_ERR_ARG, "mv_aws_matvec: y_scaled needs row scales");
+    for (int v0 = 0; v0 < batch; v0 += 16) {
+        const int nb = std::min(16, batch - v0);
+        AwrLaunch P = L;
+        P.x = x + (size_t)v0 * cols;
+        P.batch = nb;
+        P.y = y + (size_t)v0 * rows;
+        P.scales = scales;
+        P.ys = ys ? ys + (size_t)v0 * rows : nullptr;
+        if (nb == 1) rc = launch_awr<1, false, true>(P, st);
+        else if (nb == 2) rc = launch_awr<2, false, true>(P, st);
+        else if (nb <= 4) rc = launch_awr<4, false, true>(P, st);
+        else if (nb <= 8) rc = launch_awr<8, false, true>(P, st);
+        else rc = launch_awr<16, false, true>(P, st);
+        if (rc) return rc;
+    }
+    return MV_OK;
+}
+
+mv_status aws_requant(const uint32_t *comp, size_t n_words, const uint32_t *offs, const uint32_t *ppf,
+                      const uint32_t *cum, const uint32_t *prob, int rows, int cols, const int8_t *x,
+                      float scale, int8_t *out8, cudaStream_t st) {
+    AwrLaunch L{};
+    mv_status rc = awr_common(comp, n_words, offs, ppf, cum, prob, rows, cols, x, L, true);
+    if (rc) return rc;
+    if (!out8) return fail(MV_ERR_ARG, "mv_aws_matvec_requant: NULL output");
+    L.batch = 1;
+    L.out8 = out8;
+    L.scale = scale;
+    return launch_awr<1, true, true>(L, st);
 }
 
 mv_status awr_requant(const uint32_t *comp, size_t n_words, const uint32_t *offs, const uint32_t *ppf,
@@ -284,6 +352,39 @@ void mat_vec_mul_coalesced(const void *in_vector_gpu, void *out_vector_gpu, size
                                    reinterpret_cast<const int8_t *>(in_vector_gpu), scale,
                                    reinterpret_cast<int8_t *>(out_vector_gpu), 0);
     if (rc) std::fprintf(stderr, "mat_vec_mul_coalesced: %s\n", mv_last_error());
+}
+
+mv_status mv_aws_matvec(const uint32_t *compressed_dev, size_t n_words, const uint32_t *warp_offsets_dev,
+                        const uint32_t *ppf_dev, const uint32_t *ppf_cum_dev,
+                        const uint32_t *ppf_prob_dev, int rows, int cols, const int8_t *x_dev,
+                        int batch, int32_t *y_dev, const float *row_scales_dev, float *y_scaled_dev,
+                        void *stream) {
+    return mv::aws_matvec(compressed_dev, n_words, warp_offsets_dev, ppf_dev, ppf_cum_dev, ppf_prob_dev,
+                          rows, cols, x_dev, batch, y_dev, row_scales_dev, y_scaled_dev,
+                          (cudaStream_t)stream);
+}
+
+mv_status mv_aws_matvec_requant(const uint32_t *compressed_dev, size_t n_words,
+                                const uint32_t *warp_offsets_dev, const uint32_t *ppf_dev,
+                                const uint32_t *ppf_cum_dev, const uint32_t *ppf_prob_dev, int rows,
+                                int cols, const int8_t *x_dev, float scale, int8_t *out8_dev,
+                                void *stream) {
+    return mv::aws_requant(compressed_dev, n_words, warp_offsets_dev, ppf_dev, ppf_cum_dev, ppf_prob_dev,
+                           rows, cols, x_dev, scale, out8_dev, (cudaStream_t)stream);
+}
+
+// buffered/ans-warp-stripes.cu:38-60 (the launcher of the stripes program, which has the same name as the
+// rows program's; renamed here so that both live in one library): same arguments, same int8 output,
+// legacy default stream, no bounds checks (the stream length is unknown).
+void mat_vec_mul_coalesced_stripes(const void *in_vector_gpu, void *out_vector_gpu, size_t in_dim,
+                                   size_t out_dim, float scale, const void *compressed,
+                                   const uint32_t *warp_offsets, const uint32_t *ppf, const uint32_t *ppf_cum,
+                                   const uint32_t *ppf_prob) {
+    mv_status rc = mv::aws_requant(reinterpret_cast<const uint32_t *>(compressed), 0, warp_offsets, ppf,
+                                   ppf_cum, ppf_prob, (int)out_dim, (int)in_dim,
+                                   reinterpret_cast<const int8_t *>(in_vector_gpu), scale,
+                                   reinterpret_cast<int8_t *>(out_vector_gpu), 0);
+    if (rc) std::fprintf(stderr, "mat_vec_mul_coalesced_stripes: %s\n", mv_last_error());
 }
 
 }  // extern "C"

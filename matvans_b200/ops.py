@@ -119,6 +119,37 @@ class AwrMatrix(_Matrix):
         return out
 
 
+class AwsMatrix(AwrMatrix):
+    """A matrix in the reference's ans-warp-stripes layout (buffered/encoder.py:323-391): the AWR coder
+    and tables, one warp per 32-row stripe, one offset per stripe."""
+
+    @classmethod
+    def encode(cls, W, device="cuda"):
+        from . import codec
+        comp, offs, mn, cdf = codec.compress_ans_warp_stripes(W, 32)
+        p, pc, pp = codec.decoder_model_from_128bit_encoder_model(mn, cdf)
+        return cls(comp, offs, codec.pack_4bytes(p), codec.pack_4bytes(pc), codec.pack_4bytes(pp),
+                   W.shape[0], W.shape[1], device)
+
+    @property
+    def payload_bytes(self):
+        return 4 * self.n_words + 4 * (self.rows // 32) + 3 * 128
+
+    def _launch(self, x2, B, y, scales, ys):
+        check(lib().mv_aws_matvec(_p(self.compressed), self.n_words, _p(self.offsets), _p(self.ppf),
+                                  _p(self.ppf_cum), _p(self.ppf_prob), self.rows, self.cols, _p(x2), B, _p(y),
+                                  _p(scales), _p(ys), _stream()))
+
+    def matvec_requant(self, x, scale, out=None):
+        """Fused int8 output of ans-warp-stripes-kernel.cu:220-226."""
+        x2, _ = _as_x(x, self.cols, self.device)
+        out = out if out is not None else torch.empty(self.rows, dtype=torch.int8, device=self.device)
+        check(lib().mv_aws_matvec_requant(_p(self.compressed), self.n_words, _p(self.offsets), _p(self.ppf),
+                                          _p(self.ppf_cum), _p(self.ppf_prob), self.rows, self.cols, _p(x2),
+                                          ctypes.c_float(scale), _p(out), _stream()))
+        return out
+
+
 class WprMatrix(_Matrix):
     """A matrix in the reference's matvansWarpPerRow .bin layout."""
 
@@ -333,6 +364,16 @@ def mat_vec_mul_coalesced(in_vector_gpu, out_vector_gpu, in_dim, out_dim, scale,
                                 _p(ppf_prob))
     err = lib().mv_last_error().decode()
     return err
+
+
+def mat_vec_mul_coalesced_stripes(in_vector_gpu, out_vector_gpu, in_dim, out_dim, scale, compressed, warp_offsets,
+                                  ppf, ppf_cum, ppf_prob):
+    """The reference launcher of buffered/ans-warp-stripes.cu:38-60 (renamed: the rows program uses the
+    same name), on torch device tensors, legacy default stream."""
+    lib().mat_vec_mul_coalesced_stripes(_p(in_vector_gpu), _p(out_vector_gpu), int(in_dim), int(out_dim),
+                                        ctypes.c_float(scale), _p(compressed), _p(warp_offsets), _p(ppf),
+                                        _p(ppf_cum), _p(ppf_prob))
+    return lib().mv_last_error().decode()
 
 
 def requant_absmax(y, out8=None):

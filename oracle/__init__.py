@@ -49,8 +49,10 @@ def lib():
         L.orc_awr_matvec_mt.argtypes = [P, i64, P, i64, i64, P, P, P, P, ctypes.c_int, P, ctypes.c_int]
         L.orc_wpr_matvec_mt.argtypes = [P, i64, P, i64, i64, ctypes.c_int8, P, ctypes.c_int, P, P,
                                         ctypes.c_int, P, ctypes.c_int]
+        L.orc_aws_decode.argtypes = [P, i64, P, i64, i64, P, P, P, P]
+        L.orc_aws_matvec.argtypes = [P, i64, P, i64, i64, P, P, P, P, ctypes.c_int, P]
         for f in ("orc_matvec_i8", "orc_awr_decode", "orc_wpr_decode", "orc_awr_matvec_mt",
-                  "orc_wpr_matvec_mt"):
+                  "orc_wpr_matvec_mt", "orc_aws_decode", "orc_aws_matvec"):
             getattr(L, f).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -105,6 +107,28 @@ def awr_matvec(compressed, offsets, rows, cols, ppf, ppf_cum, ppf_prob, x, nthre
     y = np.empty((x2.shape[0], rows), dtype=np.int32)
     _check(lib().orc_awr_matvec_mt(_p(comp), comp.size, _p(offs), rows, cols, *[_p(a) for a in t],
                                    _p(x2), x2.shape[0], _p(y), nthreads), "awr_matvec")
+    return y if np.ndim(x) == 2 else y[0]
+
+
+def aws_decode(compressed, offsets, rows, cols, ppf, ppf_cum, ppf_prob):
+    """'ans-warp-stripes' layout (buffered/ans-warp-stripes-kernel.cu:21-227): one offset per 32-row stripe."""
+    comp = _c(compressed, np.uint32)
+    offs = _c(offsets, np.uint32)
+    t = [_c(a, np.uint32) for a in (ppf, ppf_cum, ppf_prob)]
+    W = np.empty((rows, cols), dtype=np.int8)
+    _check(lib().orc_aws_decode(_p(comp), comp.size, _p(offs), rows, cols, *[_p(a) for a in t], _p(W)),
+           "aws_decode")
+    return W
+
+
+def aws_matvec(compressed, offsets, rows, cols, ppf, ppf_cum, ppf_prob, x):
+    comp = _c(compressed, np.uint32)
+    offs = _c(offsets, np.uint32)
+    t = [_c(a, np.uint32) for a in (ppf, ppf_cum, ppf_prob)]
+    x2 = _c(np.atleast_2d(x), np.int8)
+    y = np.empty((x2.shape[0], rows), dtype=np.int32)
+    _check(lib().orc_aws_matvec(_p(comp), comp.size, _p(offs), rows, cols, *[_p(a) for a in t],
+                                _p(x2), x2.shape[0], _p(y)), "aws_matvec")
     return y if np.ndim(x) == 2 else y[0]
 
 

@@ -102,9 +102,14 @@ static inline orc_u4 awr_load_u4(const uint32_t *comp, int64_t n_words, int64_t 
  * kernel can issue when the warp cache reload lands exactly on a 128-word
  * boundary, ans-warp-rows-kernel.cu:103-111) return zeros; such words are
  * never consumed. */
-static int awr_row(const uint32_t *comp, int64_t n_words, uint32_t row_u4, int64_t cols,
-                   const uint32_t *ppf, const uint32_t *cum, const uint32_t *prob,
-                   int8_t *w_out, const int8_t *x, int batch, int64_t *acc_out)
+/* stripes = 0: one AWR row (lane l holds the quad at columns 4(j+l)..+3 of step j, all lanes feed
+ * acc_out[b]); stripes = 1: one "ans-warp-stripes" stripe of 32 rows (ans-warp-stripes-kernel.cu:21-227,
+ * layout encoder.py:323-391): lane l is row l of the stripe and decodes its quad j (columns 4j..4j+3) at
+ * step j, w_out is [32][cols] and acc_out [32][batch].  The word stream, its 128-word cache and the
+ * lane-order refills are the same in both layouts. */
+static int awr_row_x(const uint32_t *comp, int64_t n_words, uint32_t row_u4, int64_t cols,
+                     const uint32_t *ppf, const uint32_t *cum, const uint32_t *prob,
+                     int8_t *w_out, const int8_t *x, int batch, int64_t *acc_out, int stripes)
 {
     int64_t cursor = (int64_t)row_u4 * 4;   /* word index of the next 128-word block */
     if (cursor + 128 > n_words) return ORC_ERR_BOUNDS;
@@ -117,9 +122,9 @@ static int awr_row(const uint32_t *comp, int64_t n_words, uint32_t row_u4, int64
     cursor += 128;
     uint32_t wcc = 64;
     const int64_t quads = cols / 4;
-    if (acc_out) for (int b = 0; b < batch; b++) acc_out[b] = 0;
+    if (acc_out) for (int b = 0; b < (stripes ? 32 * batch : batch); b++) acc_out[b] = 0;
 
-    for (int64_t j = 0; j < quads; j += 32) {
+    for (int64_t j = 0; j < quads; j += (stripes ? 1 : 32)) {
         uint32_t ballot = 0;
         for (int l = 0; l < 32; l++)
             if ((state[l] >> 32) == 0) ballot |= 1u << l;
@@ -163,15 +168,55 @@ static int awr_row(const uint32_t *comp, int64_t n_words, uint32_t row_u4, int64
             uint32_t p01 = p[0] * p[1], p012 = p01 * p[2], p0123 = p012 * p[3];
             uint32_t ns = rem[0] + p[0] * rem[1] + p01 * rem[2] + p012 * rem[3];
             state[l] = (s >> 28) * (uint64_t)p0123 + (uint64_t)ns;
-            int64_t col = 4 * (j + l);
-            if (w_out) for (int i = 0; i < 4; i++) w_out[col + i] = sym[i];
+            const int64_t col = stripes ? 4 * j : 4 * (j + l);
+            if (w_out) for (int i = 0; i < 4; i++) w_out[(stripes ? l * cols : 0) + col + i] = sym[i];
             if (acc_out)
                 for (int b = 0; b < batch; b++) {
                     const int8_t *xb = x + (int64_t)b * cols + col;
-                    acc_out[b] += (int64_t)sym[0] * xb[0] + (int64_t)sym[1] * xb[1] +
-                                  (int64_t)sym[2] * xb[2] + (int64_t)sym[3] * xb[3];
+                    acc_out[stripes ? l * batch + b : b] +=
+                        (int64_t)sym[0] * xb[0] + (int64_t)sym[1] * xb[1] + (int64_t)sym[2] * xb[2] +
+                        (int64_t)sym[3] * xb[3];
                 }
         }
+    }
+    return ORC_OK;
+}
+
+static int awr_row(const uint32_t *comp, int64_t n_words, uint32_t row_u4, int64_t cols,
+                   const uint32_t *ppf, const uint32_t *cum, const uint32_t *prob,
+                   int8_t *w_out, const int8_t *x, int batch, int64_t *acc_out)
+{
+    return awr_row_x(comp, n_words, row_u4, cols, ppf, cum, prob, w_out, x, batch, acc_out, 0);
+}
+
+/* Decode a whole "ans-warp-stripes" matrix to int8 W[rows][cols] (rows % 32 == 0, cols % 4 == 0,
+ * buffered/encoder.py:326-327; warp_offsets: one per stripe, in uint4 units). */
+int orc_aws_decode(const uint32_t *comp, int64_t n_words, const uint32_t *warp_offsets,
+                   int64_t rows, int64_t cols, const uint32_t *ppf, const uint32_t *cum,
+                   const uint32_t *prob, int8_t *W)
+{
+    if (rows % 32 != 0 || cols % 4 != 0) return ORC_ERR_SHAPE;
+    for (int64_t s = 0; s < rows / 32; s++) {
+        int rc = awr_row_x(comp, n_words, warp_offsets[s], cols, ppf, cum, prob, W + s * 32 * cols,
+                           NULL, 0, NULL, 1);
+        if (rc) return rc;
+    }
+    return ORC_OK;
+}
+
+/* Fused "ans-warp-stripes" decode + int8 dot products (single thread): x [batch][cols], y [batch][rows]. */
+int orc_aws_matvec(const uint32_t *comp, int64_t n_words, const uint32_t *warp_offsets,
+                   int64_t rows, int64_t cols, const uint32_t *ppf, const uint32_t *cum,
+                   const uint32_t *prob, const int8_t *x, int batch, int32_t *y)
+{
+    if (rows % 32 != 0 || cols % 4 != 0) return ORC_ERR_SHAPE;
+    if (batch < 1 || batch > 64) return ORC_ERR_SHAPE;
+    int64_t acc[32 * 64];
+    for (int64_t s = 0; s < rows / 32; s++) {
+        int rc = awr_row_x(comp, n_words, warp_offsets[s], cols, ppf, cum, prob, NULL, x, batch, acc, 1);
+        if (rc) return rc;
+        for (int l = 0; l < 32; l++)
+            for (int b = 0; b < batch; b++) y[(int64_t)b * rows + s * 32 + l] = (int32_t)acc[l * batch + b];
     }
     return ORC_OK;
 }

@@ -16,6 +16,10 @@ It imports the reference's Python encoders unchanged and records their outputs:
 * ``awr_cases.npz`` -- compress_ans_warp_rows on non-square and edge-case
   matrices (single value, 128 distinct values, sigma 2, Laplace) plus the
   1024x1024 sigma-4 matrix of the plain-method workload.
+* ``aws_chain.safetensors`` / ``aws_cases.npz`` -- the same pipeline and the
+  same kinds of edge cases (rows a multiple of 32) for the "ans-warp-stripes"
+  layout, compressed with compress_ans_warp_stripes (encoder.py:323-391).
+  ``python tests/golden/gen_golden.py aws`` regenerates only these.
 * ``wpr_chain_512.bin`` -- the reference's own matvansWarpPerRow pipeline
   (create_matrices_WarpPerRow.py, seed 20250310, -w 512 -n 3 -e 5), including
   its result_hash.
@@ -137,6 +141,44 @@ def gen_awr(enc):
     np.savez_compressed(os.path.join(HERE, "awr_cases.npz"), **cases)
 
 
+def gen_aws(enc):
+    # (1) the reference's pipeline with the stripes compressor (same seed and sizes as the AWR chain)
+    np.random.seed(20250829)
+    mats, v0, scales, hashes = enc.create_rnd_matrices_and_vec(256, 3, 4.0)
+    enc.compress_all_matrices(mats, v0, scales, hashes, enc.compress_ans_warp_stripes,
+                              os.path.join(HERE, "aws_chain.safetensors"))
+
+    # (2) direct calls on edge cases (rows must be a multiple of 32, encoder.py:326)
+    rng = np.random.default_rng(4321)
+    cases = {}
+
+    def add(name, W):
+        comp, offs, min_value, cdf = enc.compress_ans_warp_stripes(W, 32)
+        ppf, pcum, pprob = enc.decoder_model_from_128bit_encoder_model(min_value, cdf)
+        cases[name + "_W"] = W
+        cases[name + "_compressed"] = comp
+        cases[name + "_offsets"] = offs
+        cases[name + "_min"] = np.array([min_value], dtype=np.int32)
+        cases[name + "_cdf"] = cdf
+        cases[name + "_ppf"] = enc.pack_4bytes(ppf)
+        cases[name + "_ppf_cum"] = enc.pack_4bytes(pcum)
+        cases[name + "_ppf_prob"] = enc.pack_4bytes(pprob)
+
+    g = lambda s, shape: np.clip(np.round(rng.normal(0, s, size=shape)), -127, 127).astype(np.int8)
+    add("s4_64x512", g(4.0, (64, 512)))
+    add("s2_32x260", g(2.0, (32, 260)))
+    add("s1_96x128", g(1.0, (96, 128)))
+    lap = np.clip(np.round(rng.laplace(0, 3.0, size=(32, 384))), -60, 60).astype(np.int8)
+    add("lap3_32x384", lap)
+    add("const_32x128", np.full((32, 128), -3, dtype=np.int8))
+    two = np.where(rng.random((32, 256)) < 0.97, 5, -7).astype(np.int8)
+    add("two_32x256", two)
+    wide = rng.integers(-64, 64, size=(32, 512)).astype(np.int8)   # exactly 128 values
+    add("wide128_32x512", wide)
+    add("s4_256x1024", g(4.0, (256, 1024)))
+    np.savez_compressed(os.path.join(HERE, "aws_cases.npz"), **cases)
+
+
 def gen_wpr(workdir):
     # (1) the reference's own pipeline: 3 square 512x512 matrices, entropy bound 5
     mod = run_wpr_script(512, 3, 5, workdir)
@@ -165,9 +207,14 @@ def gen_wpr(workdir):
 
 def main():
     enc = load_awr_encoder()
-    gen_awr(enc)
-    with tempfile.TemporaryDirectory() as d:
-        gen_wpr(d)
+    only = sys.argv[1:]
+    if not only or "awr" in only:
+        gen_awr(enc)
+    if not only or "aws" in only:
+        gen_aws(enc)
+    if not only or "wpr" in only:
+        with tempfile.TemporaryDirectory() as d:
+            gen_wpr(d)
     for fn in sorted(os.listdir(HERE)):
         if not fn.endswith(".py"):
             print(f"{fn:32s} {os.path.getsize(os.path.join(HERE, fn)):>9d} B")

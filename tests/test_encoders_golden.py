@@ -128,3 +128,33 @@ def test_shape_errors():
     wide = np.arange(-128, 128, dtype=np.int8).repeat(2).reshape(2, 256)
     with pytest.raises(MatvansError):
         codec.compress_ans_warp_rows(wide)
+
+
+def test_aws_encoder_byte_identical_on_cases():
+    z = np.load(golden("aws_cases.npz"))
+    names = sorted({k[:-2] for k in z.files if k.endswith("_W")})
+    assert len(names) >= 8
+    for name in names:
+        comp, offs, mn, cdf = codec.compress_ans_warp_stripes(z[name + "_W"], 32)
+        assert np.array_equal(comp, z[name + "_compressed"]), name
+        assert np.array_equal(offs, z[name + "_offsets"]), name
+        assert mn == int(z[name + "_min"][0]) and np.array_equal(cdf, z[name + "_cdf"]), name
+
+
+def test_compress_all_matrices_stripes_reproduces_reference_file(tmp_path):
+    raw = np.load(golden("awr_chain_raw.npz"))
+    out = tmp_path / "chain_stripes.safetensors"
+    codec.compress_all_matrices(raw["matrices"], raw["initial_vector"], raw["scales"], raw["hashes"],
+                                codec.compress_ans_warp_stripes, str(out))
+    mine = formats.read_safetensors(str(out))
+    ref = formats.read_safetensors(golden("aws_chain.safetensors"))
+    assert sorted(mine) == sorted(ref)
+    for k in ref:
+        assert mine[k].dtype == ref[k].dtype and np.array_equal(mine[k], ref[k]), k
+
+
+def test_aws_encoder_rejects_bad_shapes():
+    with pytest.raises(Exception):
+        codec.compress_ans_warp_stripes(np.zeros((48, 128), np.int8))
+    with pytest.raises(Exception):
+        codec.compress_ans_warp_stripes(np.zeros((32, 130), np.int8))

@@ -107,3 +107,47 @@ def test_wpr_plain_method_1024():
                           ref["x"], nthreads=4)
     assert np.array_equal(y, ref["y"])
     assert np.array_equal(f["vector"], ref["x"])
+
+
+# ------------------------------------------------------------ ans-warp-stripes
+
+def _aws_cases():
+    z = np.load(golden("aws_cases.npz"))
+    names = sorted({k[:-2] for k in z.files if k.endswith("_W")})
+    return {n: {k[len(n) + 1:]: z[k] for k in z.files if k.startswith(n + "_")} for n in names}
+
+
+def test_aws_cases_round_trip():
+    for name, c in _aws_cases().items():
+        W = c["W"]
+        rows, cols = W.shape
+        got = oracle.aws_decode(c["compressed"], c["offsets"], rows, cols, c["ppf"], c["ppf_cum"], c["ppf_prob"])
+        assert np.array_equal(got, W), name
+        x = np.random.default_rng(8).integers(-127, 128, size=(3, cols)).astype(np.int8)
+        y = oracle.aws_matvec(c["compressed"], c["offsets"], rows, cols, c["ppf"], c["ppf_cum"], c["ppf_prob"], x)
+        assert np.array_equal(y, oracle.matvec_i8(W, x)), name
+
+
+def test_aws_chain_decodes_and_reproduces_reference_hashes():
+    # the reference's seed-20250829 pipeline compressed with compress_ans_warp_stripes: same matrices and
+    # hashes as the rows-layout chain
+    st = formats.read_safetensors(golden("aws_chain.safetensors"))
+    raw = np.load(golden("awr_chain_raw.npz"))
+    mats = raw["matrices"]
+    count, dim = mats.shape[0], mats.shape[1]
+    assert st["all_warp_offsets"].shape == (count, dim // 32)
+    v = st["initial_vector"]
+    for k in range(count):
+        W = oracle.aws_decode(st["compressed"], st["all_warp_offsets"][k], dim, dim,
+                              st["all_ppfs"][k], st["all_ppfs_cum"][k], st["all_ppfs_prob"][k])
+        assert np.array_equal(W, mats[k]), f"matrix {k} does not round-trip"
+        y = oracle.aws_matvec(st["compressed"], st["all_warp_offsets"][k], dim, dim,
+                              st["all_ppfs"][k], st["all_ppfs_cum"][k], st["all_ppfs_prob"][k], v)
+        v = np.round(y * st["scales"][k]).astype(np.int8)  # the reference's requantisation, encoder.py:46-51
+        assert oracle.hash_int8(v) == int(st["hashes"][k]), k
+
+
+def test_aws_rejects_bad_shape():
+    c = _aws_cases()["s4_64x512"]
+    with pytest.raises(oracle.OracleError):
+        oracle.aws_decode(c["compressed"], c["offsets"], 48, 512, c["ppf"], c["ppf_cum"], c["ppf_prob"])
