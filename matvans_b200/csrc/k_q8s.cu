@@ -1431,6 +1431,15 @@ void plan_job(Q8Job &J, const mv_q8_tuning &t, uint32_t &item, int parts) {
 
 }  // namespace
 
+// Work items per stripe for a single matrix: enough items for ~4 per SM, but no more than it takes
+// to give each of the CTA's sg = warps x ilp segment slots one segment per item (ceil, so that the
+// items of a stripe are as even as its segment count allows)
+int default_parts(int nseg, int sg, int stripes) {
+    const int fill = (4 * sm_count() + stripes - 1) / stripes;
+    const int even = (nseg + sg - 1) / sg;
+    return std::max(1, std::min(fill, even));
+}
+
 bool q8s_supports(const mv_q8_view *m, const int8_t *x) {
     return (m->cols & 15) == 0 && ((uintptr_t)x & 15) == 0 && (m->seg_quads & 3) == 0;
 }
@@ -1454,7 +1463,7 @@ mv_status q8s_matvec(const mv_q8_view *m, const int8_t *x, int batch, int32_t *y
         // a single matrix: split stripes so that every warp slot of the GPU gets work
         const int stripes = (m->rows + 31) / 32;
         const int sg = t.warps * t.ilp;
-        int parts = t.parts > 0 ? t.parts : std::max(1, std::min(m->nseg / sg, (3 * sm_count() + stripes - 1) / stripes));
+        int parts = t.parts > 0 ? t.parts : default_parts(m->nseg, sg, stripes);
         plan_job(L.job0, t, items, parts);
         if (L.job0.atomic) L.job0.ys = nullptr;
         L.jobs = nullptr;
@@ -1506,7 +1515,7 @@ mv_status q8f_run(const mv_q8_view *m, int mode, const uint16_t *in, int batch, 
         int parts = 1;
         if (mode == 2) {
             const int stripes = (m->rows + 31) / 32, sg = t.warps * t.ilp;
-            parts = t.parts > 0 ? t.parts : std::max(1, std::min(m->nseg / sg, (3 * sm_count() + stripes - 1) / stripes));
+            parts = t.parts > 0 ? t.parts : default_parts(m->nseg, sg, stripes);
         }
         plan_job(L.job0, t, items, parts);
         if (mode == 1 && L.job0.atomic) return fail(MV_ERR_ARG, "float forward needs whole stripes (parts = 1)");
