@@ -36,6 +36,9 @@ SIGMAS = [4.0, 2.0]
 METRIC = "us/matvec & int8-equiv GB/s vs dense dp4a int8 on B200, bit-exact int32 output"
 UNIT = "GB/s"
 L2_BYTES = 126 * 2 ** 20
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the step's kernel (q8s_kernel, 4 warps, ilp 1),
+# from an ncu --set full capture of `bench.py --profile --tuning 4,1,1,0,0,0`
+STEP_DRAM_BYTES = 215.6e6
 
 
 def gen_matrix(shape, sigma, seed):
@@ -683,7 +686,8 @@ def run_ours(args):
             "speedup_vs_dense_dp4a": {k: round(dense[k.split("_s")[0]]["us"] / v["us"], 3)
                                       for k, v in per.items() if k.split("_s")[0] in dense and "_s4_" in k},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": STEP_DRAM_BYTES, "traffic_unit": "bytes per launch",
+                         "algorithmic_bytes": alg, "peak_kind": peak_kind,
                          "kernel": "q8s_kernel<1,ILP,DEPTH> (mv_q8_stack_matvec)",
                          "note": "algorithmic bytes = compressed streams + tables + offsets + x + int32 y"},
             "gpu_launches": args.steps * 3,
