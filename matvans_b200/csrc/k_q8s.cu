@@ -231,7 +231,7 @@ struct IntCons {
     static constexpr int kNV = NV;
     static constexpr int kRedNV = NV;
     static constexpr int kMinCtas = 1;
-    static constexpr int kMaxThreads = 256;
+    static constexpr int kMaxThreads = 512;  // up to 16 warps per CTA
     static constexpr int kTmemCols = 0;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }

@@ -316,8 +316,9 @@ class Q8Chain:
             raise ValueError("batch must be 1..16")
         if len(scales) != len(self.matrices):
             raise ValueError("one scale per matrix")
-        # a chain launch is cooperative, one CTA per SM on the tensor cores: 16 warps fill the SM there
-        default = (16, 1, 1, 0) if self.batch >= 8 else (0, 0, 0, 0)
+        # a chain launch is cooperative (one CTA per SM on the tensor cores) and each step's work items are
+        # whole stripes: 16-warp CTAs give each stripe the most warps
+        default = (16, 1, 1, 0)
         self.tuning = tuning if isinstance(tuning, Q8Tuning) else Q8Tuning(*(tuning or default))
         self.scales = torch.tensor([float(s) for s in scales], dtype=torch.float32, device=self.device)
         self.xs = [x0 if x0 is not None else torch.zeros((self.batch, self.matrices[0].cols), dtype=torch.int8,

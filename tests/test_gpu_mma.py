@@ -71,8 +71,9 @@ def test_mma_segment_lengths(seg_quads):
 
 def test_launches_that_do_not_fit_are_rejected():
     M = ops.Q8Matrix.encode(np.ones((64, 512), np.int8))
-    with pytest.raises(_lib.MatvansError):  # the CUDA-core engine takes at most 8 warps per CTA
-        M.matvec(torch.ones((16, 512), dtype=torch.int8), tuning=(16, 1, 1, 0, 0, DP4A))
+    with pytest.raises(_lib.MatvansError):  # the CUDA-core float consumers take at most 8 warps per CTA
+        M.matvec_bf16(torch.ones((1, 512), dtype=torch.bfloat16, device="cuda"),
+                      torch.ones(64, device="cuda"), tuning=(16, 1, 1, 0, 0, DP4A))
     W = np.random.default_rng(1).integers(-127, 128, size=(96, 1520)).astype(np.int8)  # ~8 bits/weight
     M = ops.Q8Matrix.encode(W, local=True, seg_quads=128)
     with pytest.raises(_lib.MatvansError):  # 16 warps of 128-quad stream buffers exceed shared memory
