@@ -629,6 +629,12 @@ struct MmaCons {
     // lane (b, h) holds 16 bytes (column half h) of vector b for each 32-column piece of a window
     __device__ __forceinline__ void load_window(uint4 (&xr)[kXChunks], const int8_t *xrow, bool xok, int colbase,
                                                 int pbase, int npieces) const {
+        if (xok && pbase + kXChunks <= npieces && colbase + 32 * (pbase + kXChunks - 1) < cols) {
+            // a full window inside the row: plain loads, no per-piece checks
+#pragma unroll
+            for (int i = 0; i < kXChunks; i++) xr[i] = ldx_u4(xrow + 32 * (pbase + i));
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < kXChunks; i++) {
             const int c = pbase + i;
@@ -671,13 +677,13 @@ struct MmaCons {
             wait_mma(L);
             const int pw = p & (kXChunks - 1);  // piece within the window
             if (pw == 0) {
-                const int cn = min(kXChunks, npieces - p);
+                // the whole window is stored (pieces past the segment hold zeros or stale x, and are never
+                // multiplied: the MMAs of a pair read only the pieces that exist)
 #pragma unroll
                 for (int i = 0; i < kXChunks; i++)
-                    if (i < cn)
-                        asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 512u),
-                                     "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
-                                     : "memory");
+                    asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 512u),
+                                 "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
+                                 : "memory");
                 fence_proxy_async_smem();  // the x tile is read by the tensor core (async proxy)
                 if (p + kXChunks < npieces) load_window(xr, xrow, xok, colbase, p + kXChunks, npieces);
             }
