@@ -12,6 +12,7 @@ GPU name, driver, library build, shape, table mode, segment length, bits per
 weight and batch, in $MATVANS_AUTOTUNE_CACHE (default
 ~/.cache/matvans_b200/autotune.json).
 """
+import fcntl
 import json
 import os
 import threading
@@ -55,11 +56,26 @@ def _load():
 
 def _store(db):
     p = cache_path()
-    os.makedirs(os.path.dirname(p), exist_ok=True)
+    os.makedirs(os.path.dirname(p) or ".", exist_ok=True)
     tmp = p + f".tmp{os.getpid()}"
     with open(tmp, "w") as f:
         json.dump(db, f, indent=1, sort_keys=True)
     os.replace(tmp, p)
+
+
+def _update(k, entry):
+    """Adds one entry under an exclusive lock on <cache>.lock, so that processes tuning at the same time
+    (one per GPU) keep each other's entries; the file itself is replaced atomically."""
+    p = cache_path()
+    os.makedirs(os.path.dirname(p) or ".", exist_ok=True)
+    with _lock, open(p + ".lock", "a+") as lf:
+        fcntl.flock(lf, fcntl.LOCK_EX)
+        try:
+            db = _load()
+            db[k] = entry
+            _store(db)
+        finally:
+            fcntl.flock(lf, fcntl.LOCK_UN)
 
 
 def _build_id():
@@ -132,10 +148,7 @@ def tune(M, batch=1, candidates=None, reps=10, force=False):
         raise RuntimeError("autotune: no candidate launched")
     best = min(results, key=results.get)
     entry = {"tuning": [int(v) for v in best.split(",")], "us": results[best], "all": results, "copies": R}
-    with _lock:
-        db = _load()
-        db[k] = entry
-        _store(db)
+    _update(k, entry)
     return Q8Tuning(*entry["tuning"]), entry
 
 
