@@ -227,7 +227,11 @@ mv_status mv_q8_matvec_tuned(const mv_q8_view *m, const int8_t *x_dev, int batch
 
 /* One matrix of a batched launch: the matrix, its input x [batch][cols] and
  * outputs y [batch][rows] (+ optional scaled output).  ngroups, atomic and
- * item0 are filled in by mv_q8_stack_plan. */
+ * item0 are filled in by mv_q8_stack_plan.  x_tiles (optional, NULL for none)
+ * is device scratch of mv_q8_x_tiles_bytes(&m) bytes, 16-byte aligned: with
+ * 8..16 vectors on the tensor cores, mv_q8_stack_matvec first lays x out there
+ * in the MMA operand layout, and each warp then brings its x windows in with
+ * one asynchronous bulk copy instead of per-lane loads and stores. */
 typedef struct mv_q8_job {
     mv_q8_view m;
     const int8_t *x;
@@ -238,7 +242,12 @@ typedef struct mv_q8_job {
     int32_t atomic;
     uint32_t item0;
     uint32_t pad;
+    int8_t *x_tiles;
 } mv_q8_job;
+
+/* Bytes of the x_tiles scratch of a job on matrix m: one 2 KB tile (16
+ * vectors x 128 columns) per 32 quads of every segment. */
+size_t mv_q8_x_tiles_bytes(const mv_q8_view *m);
 
 typedef struct mv_q8_stack_info {
     uint32_t nitems;          /* work items (matrix, 32-row stripe, segment group) */

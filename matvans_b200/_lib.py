@@ -26,6 +26,7 @@ EXPORTS = [
     "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc", "mv_q8_matvec_tuned", "mv_q8_stack_plan",
     "mv_q8_stack_matvec", "mv_q8_matvec_bf16", "mv_q8_matvec_t_bf16", "mv_q8_chain_plan", "mv_q8_chain_matvec",
     "mv_aws_matvec", "mv_aws_matvec_requant", "mv_aws_encode", "mat_vec_mul_coalesced_stripes",
+    "mv_q8_x_tiles_bytes",
 ]
 
 
@@ -54,7 +55,7 @@ class Q8Job(ctypes.Structure):
     """struct mv_q8_job."""
     _fields_ = [("m", Q8View), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("scales", ctypes.c_void_p),
                 ("ys", ctypes.c_void_p), ("ngroups", ctypes.c_int32), ("atomic", ctypes.c_int32),
-                ("item0", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+                ("item0", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("x_tiles", ctypes.c_void_p)]
 
 
 class Q8StackInfo(ctypes.Structure):
@@ -93,6 +94,7 @@ def lib():
         "mv_q8_matvec_tuned": ([ctypes.POINTER(Q8View), P, i32, P, P, P, ctypes.POINTER(Q8Tuning), P], st),
         "mv_q8_stack_plan": ([ctypes.POINTER(Q8Job), i32, ctypes.POINTER(Q8Tuning), ctypes.POINTER(Q8StackInfo)], st),
         "mv_q8_stack_matvec": ([P, i32, ctypes.POINTER(Q8StackInfo), i32, ctypes.POINTER(Q8Tuning), P], st),
+        "mv_q8_x_tiles_bytes": ([ctypes.POINTER(Q8View)], sz),
         "mv_q8_chain_plan": ([ctypes.POINTER(Q8Job), i32, ctypes.POINTER(Q8Tuning), ctypes.POINTER(Q8StackInfo)], st),
         "mv_q8_chain_matvec": ([P, i32, ctypes.POINTER(Q8StackInfo), i32, P, P, ctypes.POINTER(Q8Tuning), P], st),
         "mv_q8_matvec_bf16": ([ctypes.POINTER(Q8View), P, i32, P, P, ctypes.POINTER(Q8Tuning), P], st),

@@ -561,21 +561,24 @@ struct MmaCons {
     static constexpr int kXChunks = 4;    // x tile: 4 pieces of 32 columns x 16 vectors (512 B each)
     static constexpr int kXBytes = kXChunks * 512;
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
-        // x tile 2 KB per warp, one mbarrier per warp, TMEM address slot (the last 128 bytes); a multiple
-        // of 128 bytes, so the stream buffers that follow stay 16-byte aligned for the bulk copies
-        return (((size_t)W * kXBytes + (size_t)W * 8 + 128) + 127) / 128 * 128;
+        // two x tiles of 2 KB per warp, three mbarriers per warp (MMA commits, x copies into tile 0 / 1),
+        // TMEM address slot (the last 128 bytes); a multiple of 128 bytes, so the stream buffers that
+        // follow stay 16-byte aligned for the bulk copies
+        return (((size_t)W * 2 * kXBytes + (size_t)W * 24 + 128) + 127) / 128 * 128;
     }
     // the decode tables are staged in the x tiles when they fit
-    static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)W * kXBytes; }
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)W * 2 * kXBytes; }
     static __host__ __device__ constexpr uint32_t tmem_cols(int W) {
         return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : W <= 8 ? 256 : 512;
     }
-    uint32_t xt, d_tmem, st_addr, ld_addr, ncommit;
+    uint32_t xt, d_tmem, st_addr, ld_addr, ncommit, xcur, xcnt0, xcnt1;
     uint64_t b_desc0;
-    uint64_t *mbar;
+    uint64_t *mbar, *xbar;
     int *xbase;
+    unsigned char *xt_ptr;
     const int8_t *x;
-    int cols, batch, job_idx;
+    const int8_t *tiles;  // x laid out per (segment, window) by q8s_build_x_tiles, or null
+    int cols, batch, job_idx, nwin;
     bool any;
 
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int,
@@ -585,9 +588,15 @@ struct MmaCons {
         const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
         const uint32_t base = smem_u32(extra);
         xbase = reinterpret_cast<int *>(extra);
-        xt = base + (uint32_t)warp * (uint32_t)kXBytes;
-        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * kXBytes) + warp;
-        if (lane == 0) mbar_init(mbar, 1);
+        xt = base + (uint32_t)warp * (uint32_t)(2 * kXBytes);
+        xt_ptr = extra + (size_t)warp * 2 * kXBytes;
+        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 2 * kXBytes) + warp;
+        xbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 2 * kXBytes + (size_t)W * 8) + 2 * warp;
+        if (lane == 0) {
+            mbar_init(mbar, 1);
+            mbar_init(&xbar[0], 1);
+            mbar_init(&xbar[1], 1);
+        }
         fence_mbar_init();
         __syncwarp();
         // TMEM addresses: lane in bits [16,32), column in [0,16); a warp may touch only the 32 lanes of its
@@ -598,6 +607,8 @@ struct MmaCons {
         ld_addr = d_tmem + quarter;
         b_desc0 = umma_smem_desc(xt, 128u, 256u);
         ncommit = 0;
+        xcur = 1;  // the x tile of the latest window; a segment's first window goes to the other one
+        xcnt0 = xcnt1 = 0;
     }
     __device__ __forceinline__ void begin_item(const Q8SLaunch &L, const Q8Job &J, int, int, int job) {
         x = J.x;
@@ -605,6 +616,26 @@ struct MmaCons {
         batch = L.batch;
         any = false;
         job_idx = job;
+        tiles = J.x_tiles;
+        nwin = (J.m.seg_quads + 31) / 32;
+    }
+    // Bulk copy (async proxy, one lane) of x window w of segment seg into tile t; every lane counts it.
+    // The tile's previous readers (MMAs) are done, and generic writes to it (reduction area, table
+    // staging) were fenced by every writer before the CTA barrier that ended them.
+    __device__ __forceinline__ void x_copy(int t, int seg, int w, int lane) {
+        if (lane == 0) {
+            mbar_arrive_expect_tx(&xbar[t], (uint32_t)kXBytes);
+            bulk_g2s(xt_ptr + (size_t)t * kXBytes, tiles + ((size_t)seg * nwin + w) * kXBytes, (uint32_t)kXBytes,
+                     &xbar[t]);
+        }
+        if (t) xcnt1++;
+        else xcnt0++;
+    }
+    __device__ __forceinline__ void x_wait(const Q8SLaunch &L, int t) {
+        const uint32_t n = t ? xcnt1 : xcnt0;
+        // on a timeout (flagged) wait once more, bounded, so that no copy is left in flight
+        if (!mbar_wait_bounded(&xbar[t], (n - 1) & 1, L.status, L.spin_limit))
+            mbar_wait_bounded(&xbar[t], (n - 1) & 1, nullptr, L.spin_limit);
     }
     // wait until every MMA issued so far completed (the latest commit covers all earlier MMAs)
     __device__ __forceinline__ bool wait_mma(const Q8SLaunch &L) {
@@ -616,10 +647,11 @@ struct MmaCons {
         __syncwarp();
         if (elect_one()) {
             tcgen05_fence_after();
-            // B descriptor start addresses are in 16-byte units: x piece p is 512 B into the x tile
+            // B descriptor start addresses are in 16-byte units: tile xcur is 2 KB in, piece p 512 B
             const uint32_t idesc = umma_idesc_i8(128, 16);
-            umma_i8_ts(d_tmem, d_tmem + 16u, b_desc0 + (uint64_t)(piece * 32), idesc, any ? 1u : 0u);
-            if (two) umma_i8_ts(d_tmem, d_tmem + 24u, b_desc0 + (uint64_t)(piece * 32 + 32), idesc, 1u);
+            const uint64_t bd = b_desc0 + (uint64_t)(xcur * (kXBytes / 16) + piece * 32);
+            umma_i8_ts(d_tmem, d_tmem + 16u, bd, idesc, any ? 1u : 0u);
+            if (two) umma_i8_ts(d_tmem, d_tmem + 24u, bd + 32u, idesc, 1u);
             umma_commit(mbar);
         }
         __syncwarp();
@@ -658,7 +690,15 @@ struct MmaCons {
         const int8_t *xrow = x + (size_t)(xok ? b : 0) * cols + colbase;
         const uint32_t xdst = xt + (uint32_t)(b >> 3) * 256u + (uint32_t)h * 128u + (uint32_t)(b & 7) * 16u;
         uint4 xr[kXChunks];
-        load_window(xr, xrow, xok, colbase, 0, npieces);
+        // with x tiles: the first window goes to the tile the latest window did not use (its MMAs completed
+        // before the latest window started); without: windows pass through registers into tile 0
+        int xnext = xcur ^ 1u;
+        if (tiles) {
+            x_copy(xnext, seg0, 0, lane);
+        } else {
+            xcur = 0;
+            load_window(xr, xrow, xok, colbase, 0, npieces);
+        }
         uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
         const uint32_t kend = rows_now[0] * 32 + lane;
         // pieces in pairs: piece p = 2 * pair (+1); a window holds 2 pairs
@@ -676,7 +716,16 @@ struct MmaCons {
             // the previous pair of MMAs is done with the A tile (and, at a window start, with the x tile)
             wait_mma(L);
             const int pw = p & (kXChunks - 1);  // piece within the window
-            if (pw == 0) {
+            if (pw == 0 && tiles) {
+                // this window's copy has landed (it was the only one in flight); the next goes to the other
+                // tile, whose MMAs are done (above)
+                x_wait(L, xnext);
+                xcur = xnext;
+                if (p + kXChunks < npieces) {
+                    xnext = xcur ^ 1u;
+                    x_copy(xnext, seg0, (p + kXChunks) / kXChunks, lane);
+                }
+            } else if (pw == 0) {
                 // the whole window is stored (pieces past the segment hold zeros or stale x, and are never
                 // multiplied: the MMAs of a pair read only the pieces that exist)
 #pragma unroll
@@ -718,8 +767,9 @@ struct MmaCons {
 #pragma unroll
             for (int v = 0; v < 16; v++) r[v] = 0;
         }
-        // this warp's MMAs are complete, so its own x tile (2 KB) takes its partial sums: [vector][stripe row]
-        int *red = xbase + warp * (kXBytes / 4);
+        // this warp's MMAs (and x copies) are complete, so its own x tiles take its partial sums:
+        // [vector][stripe row]
+        int *red = xbase + warp * (2 * kXBytes / 4);
 #pragma unroll
         for (int v = 0; v < 16; v++) red[v * 32 + lane] = (int)r[v];
         tcgen05_fence_before();
@@ -728,7 +778,7 @@ struct MmaCons {
         for (int t = threadIdx.x; t < 16 * 32; t += blockDim.x) {
             const int v = t >> 5, l = t & 31;
             int sum = 0;
-            for (int w = 0; w < W; w++) sum += xbase[w * (kXBytes / 4) + t];
+            for (int w = 0; w < W; w++) sum += xbase[w * (2 * kXBytes / 4) + t];
             const int row = stripe * 32 + l;
             if (row < m.rows && v < L.batch) {
                 int32_t *dst = J.y + (size_t)v * m.rows + row;
@@ -741,6 +791,7 @@ struct MmaCons {
                 }
             }
         }
+        fence_proxy_async_smem();  // these generic accesses come before later bulk copies into the tiles
         __syncthreads();  // the x tiles are written again (tables, x) by the next item
     }
     __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_mma(L); }
@@ -1210,6 +1261,7 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
                 for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) lut[q * 32 + lane] = 1u;
                 atomicOr(L.status, MV_DEV_BAD_TABLE);
             }
+            fence_proxy_async_smem();  // the table staging may share memory with later bulk copies
             __syncthreads();
             lut_job = I.job;
             lut_stripe = I.stripe;
@@ -1265,6 +1317,30 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
 }  // namespace mv
 
 namespace mv {
+
+// x of every job with x_tiles, laid out per (segment, 32-quad window) in the tensor-core consumer's x tile
+// layout: 2 KB per tile = 4 pieces of 32 columns; piece = 2 groups of 8 vectors (256 B); group = 2 column
+// halves (128 B); half = 8 vectors x 16 bytes.  Vectors past the batch and columns past the row are zero.
+__global__ void q8s_build_x_tiles(const Q8Job *jobs, int njobs, int batch) {
+    for (int j = blockIdx.y; j < njobs; j += gridDim.y) {
+        const Q8Job &J = jobs[j];
+        if (!J.x_tiles) continue;
+        const mv_q8_view &m = J.m;
+        const int nwin = (m.seg_quads + 31) / 32;
+        const size_t units = (size_t)m.nseg * nwin * 128;  // 16-byte units
+        for (size_t u = blockIdx.x * (size_t)blockDim.x + threadIdx.x; u < units; u += (size_t)gridDim.x * blockDim.x) {
+            const size_t tile = u >> 7;
+            const int o = (int)(u & 127);
+            const int sg = (int)(tile / nwin), w = (int)(tile % nwin);
+            const int i = o >> 5, g = (o >> 4) & 1, h = (o >> 3) & 1, r = o & 7;
+            const int v = 8 * g + r;
+            const int col = 4 * sg * m.seg_quads + 128 * w + 32 * i + 16 * h;  // a multiple of 16
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (v < batch && col < m.cols) val = *reinterpret_cast<const uint4 *>(J.x + (size_t)v * m.cols + col);
+            *reinterpret_cast<uint4 *>(J.x_tiles + tile * 2048 + (size_t)o * 16) = val;
+        }
+    }
+}
 
 __global__ void q8s_zero_atomic_y(const Q8Job *jobs, int njobs, int batch) {
     for (int j = blockIdx.y; j < njobs; j += gridDim.y) {
@@ -1592,6 +1668,11 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
     return MV_OK;
 }
 
+size_t mv_q8_x_tiles_bytes(const mv_q8_view *m) {
+    if (!m || m->nseg <= 0 || m->seg_quads <= 0) return 0;
+    return (size_t)m->nseg * (size_t)((m->seg_quads + 31) / 32) * 2048;
+}
+
 mv_status mv_q8_chain_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning, mv_q8_stack_info *info) {
     if (!jobs || njobs <= 0 || !info) return mv::fail(MV_ERR_ARG, "mv_q8_chain_plan: bad arguments");
     for (int j = 0; j + 1 < njobs; j++)
@@ -1658,6 +1739,10 @@ mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_s
     dim3 zg(64, std::min(njobs, 1024));
     mv::q8s_zero_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
     MV_CUDA_TRY(cudaGetLastError(), "q8s_zero_atomic_y launch");
+    if (mv::nv_round(batch) >= 8 && t.engine == MV_ENGINE_AUTO) {  // the tensor-core consumer reads x tiles
+        mv::q8s_build_x_tiles<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
+        MV_CUDA_TRY(cudaGetLastError(), "q8s_build_x_tiles launch");
+    }
     rc = mv::launch_q8s(L, mv::nv_round(batch), t, st);
     if (rc) return rc;
     mv::q8s_scale_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);

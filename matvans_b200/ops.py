@@ -274,6 +274,9 @@ class Q8Stack:
                     for M in self.matrices] if scales is not None else None
         n = len(self.matrices)
         jobs = (Q8Job * n)()
+        # 8..16 vectors on the tensor cores: x is laid out in tiles first (device scratch per matrix)
+        use_tiles = self.batch >= 8 and self.tuning.engine == 0
+        self.x_tiles = []
         for i, M in enumerate(self.matrices):
             x = self.xs[i]
             if x.dtype != torch.int8 or tuple(x.shape) != (self.batch, M.cols) or not x.is_contiguous():
@@ -281,6 +284,11 @@ class Q8Stack:
             jobs[i].m = M.view()
             jobs[i].x = x.data_ptr()
             jobs[i].y = self.ys[i].data_ptr()
+            if use_tiles:
+                nb = lib().mv_q8_x_tiles_bytes(ctypes.byref(jobs[i].m))
+                t = torch.empty(nb, dtype=torch.uint8, device=self.device)
+                self.x_tiles.append(t)
+                jobs[i].x_tiles = t.data_ptr()
             if scales is not None:
                 jobs[i].scales = scales[i].data_ptr()
                 jobs[i].ys = self.yss[i].data_ptr()
