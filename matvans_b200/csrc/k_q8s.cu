@@ -12,9 +12,13 @@
 //     with 1-D bulk copies (cp.async.bulk, TMA engine, no multicast) completing
 //     on an mbarrier; with DEPTH = 2 the copies of the CTA's next item are in
 //     flight while the current one is decoded;
-//   * the decode table (256 quantiles x 32 lanes, entry (q,l) at word q*32+l,
-//     conflict-free) is rebuilt only when the table changes: every item for
-//     per-row tables, once per job for a global table;
+//   * the decode table (256 quantiles x 32 lanes, conflict-free) is rebuilt
+//     only when the table changes: every item for per-row tables, once per
+//     job for a global table.  CUDA-core consumers use the wide layout, 8-byte
+//     entries {f | sym << 16, r} at byte q*256 + l*8 (64 KB): one byte permute
+//     of the state gives a lookup address and r needs no extraction.  The
+//     tensor-core consumers, two CTAs per SM, keep the narrow layout, 4-byte
+//     entries f | sym << 16 | r << 24 at word q*32 + l (32 KB);
 //   * x is read through L1 with broadcast loads (all lanes of a warp read the
 //     same quad), so it needs no staging;
 //   * per-row partial sums are reduced across warps in shared memory and
@@ -219,6 +223,46 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
     return __byte_perm(__byte_perm(e0, e1, 0x0062), __byte_perm(e2, e3, 0x0062), 0x5410);
 }
 
+// The same step over the wide table: 8-byte entries {f | sym << 16, r} at byte q*256 + lane*8 from the
+// start of shared memory.  A quantile byte of the state lands in bits 8..15 of the address and lane*8 in
+// bits 0..7, so one byte permute forms each lookup address, and r arrives as a clean word.
+__device__ __forceinline__ uint32_t q8_step_wide(uint32_t &lo, uint32_t &hi, uint32_t &kidx, const uint32_t kend,
+                                                 const uint32_t *buf, const unsigned char *lut_b, uint32_t lane8,
+                                                 uint32_t &P) {
+    const uint32_t w = buf[kidx];
+    const bool need = hi == 0;
+    hi = need ? lo : hi;
+    lo = need ? w : lo;
+    kidx = need ? min(kidx + 32, kend) : kidx;
+    const uint2 e0 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5504));
+    const uint2 e1 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5514));
+    const uint2 e2 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5524));
+    const uint2 e3 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5534));
+    const uint32_t t2 = __dp2a_lo(e3.y, e2.x, e2.y);  // r2 + f2*r3
+    const uint32_t t1 = __dp2a_lo(t2, e1.x, e1.y);    // r1 + f1*t2  (t2 < 2^16)
+    const uint32_t p01 = __dp2a_lo(e1.x, e0.x, 0u);   // f1*f0 + sym1*0
+    const uint32_t p23 = __dp2a_lo(e3.x, e2.x, 0u);   // f3*f2
+    P = p01 * p23;
+    const uint32_t t0 = e0.y + (e0.x & 0xFFu) * t1;
+    const unsigned long long s = (unsigned long long)hi * P + t0;
+    lo = (uint32_t)s;
+    hi = (uint32_t)(s >> 32);
+    return __byte_perm(__byte_perm(e0.x, e1.x, 0x0062), __byte_perm(e2.x, e3.x, 0x0062), 0x5410);
+}
+
+// One step through whichever table layout the consumer uses; lut is the table base (wide) or the
+// lane's column (narrow).
+template <bool kWide>
+__device__ __forceinline__ uint32_t q8_step_t(uint32_t &lo, uint32_t &hi, uint32_t &kidx, const uint32_t kend,
+                                              const uint32_t *buf, const uint32_t *lut, uint32_t stride, int lane,
+                                              uint32_t &P) {
+    if constexpr (kWide)
+        return q8_step_wide(lo, hi, kidx, kend, buf, reinterpret_cast<const unsigned char *>(lut),
+                            (uint32_t)lane << 3, P);
+    else
+        return q8_step(lo, hi, kidx, kend, buf, lut, stride, P);
+}
+
 // --------------------------------------------------------------- consumers
 // A consumer turns decoded quads (four int8 weights of the lane's row) into
 // the kernel's output.  Per item it is set up (begin_item), fed groups of four
@@ -233,6 +277,7 @@ struct IntCons {
     static constexpr int kMinCtas = 1;
     static constexpr int kMaxThreads = 512;  // up to 16 warps per CTA
     static constexpr int kTmemCols = 0;
+    static constexpr bool kWideLut = true;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
@@ -310,6 +355,7 @@ struct FwdCons {
     static constexpr int kMinCtas = 1;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
+    static constexpr bool kWideLut = true;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
@@ -396,6 +442,7 @@ struct BwdCons {
     static constexpr int kMinCtas = 1;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
+    static constexpr bool kWideLut = true;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
@@ -485,14 +532,14 @@ __device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view
             cons.load_group(gb, q0B + iA);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
-                const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+                const uint32_t wa = q8_step_t<Cons::kWideLut>(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, lane, PA);
+                const uint32_t wb = q8_step_t<Cons::kWideLut>(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, lane, PB);
                 cons.use(ga, j, q0A + iA + j, wa, lane);
                 cons.use(gb, j, q0B + iA + j, wb, lane);
             }
         }
         for (int j = iA; j < nqB; j++) {
-            const uint32_t wb = q8_step(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, PB);
+            const uint32_t wb = q8_step_t<Cons::kWideLut>(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, lane, PB);
             cons.single(q0B + j, wb, lane);
         }
         if (nqB > 0 && (hiB != 0 || loB != PB)) atomicOr(L.status, MV_DEV_FINAL_STATE);
@@ -502,12 +549,12 @@ __device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view
         cons.load_group(ga, q0A + iA);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+            const uint32_t wa = q8_step_t<Cons::kWideLut>(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, lane, PA);
             cons.use(ga, j, q0A + iA + j, wa, lane);
         }
     }
     for (; iA < nqA; iA++) {
-        const uint32_t wa = q8_step(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, PA);
+        const uint32_t wa = q8_step_t<Cons::kWideLut>(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, lane, PA);
         cons.single(q0A + iA, wa, lane);
     }
     if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
@@ -558,6 +605,7 @@ struct MmaCons {
     static constexpr int kMinCtas = 1;    // with up to 16 warps: at most 128 registers per thread
     static constexpr int kMaxThreads = 512;  // 1 x 16 or 2 x 8 warps per SM
     static constexpr int kTmemCols = 1;   // > 0: the kernel allocates TMEM
+    static constexpr bool kWideLut = false;  // two CTAs per SM: the 32 KB table
     static constexpr int kXChunks = 4;    // x tile: 4 pieces of 32 columns x 16 vectors (512 B each)
     static constexpr int kXBytes = kXChunks * 512;
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
@@ -834,6 +882,7 @@ struct FwdMma {
     static constexpr int kMinCtas = 2;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
+    static constexpr bool kWideLut = false;
     static constexpr int kXPieces = 2;
     static constexpr int kXBytes = kXPieces * 1024;
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
@@ -1006,6 +1055,7 @@ struct BwdMma {
     static constexpr int kMinCtas = 2;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
+    static constexpr bool kWideLut = false;
     static constexpr int kGBytes = 4096;  // [hi, lo][K step 0, 1] x 1 KB
     static constexpr int kWBytes = 2048;  // W tile per warp: 2 K steps x 1 KB
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
@@ -1173,8 +1223,10 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = blockDim.x >> 5;
 
-    uint32_t *lut = reinterpret_cast<uint32_t *>(smem);                                 // 8192 words
-    unsigned char *extra = smem + 256 * 32 * 4;                                          // consumer region
+    // decode table at the start of shared memory: 256 quantiles x 32 lanes of 4 B (narrow) or 8 B (wide)
+    constexpr int kLutBytes = Cons::kWideLut ? 256 * 32 * 8 : 256 * 32 * 4;
+    uint32_t *lut = reinterpret_cast<uint32_t *>(smem);
+    unsigned char *extra = smem + kLutBytes;                                             // consumer region
     uint32_t *bufs = reinterpret_cast<uint32_t *>(extra + Cons::extra_bytes(W));         // [W][DEPTH][ILP][buf]
     int *red = reinterpret_cast<int *>(bufs + (size_t)W * DEPTH * ILP * L.buf_words);    // [W][NV][32]
     uint64_t *bars = reinterpret_cast<uint64_t *>(red + W * NV * 32);                    // [W][DEPTH]
@@ -1223,7 +1275,7 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
 
     int lut_job = -1, lut_stripe = -1;
     uint32_t consumed = 0;
-    const uint32_t *lut_l = lut + lane;
+    const uint32_t *lut_l = Cons::kWideLut ? lut : lut + lane;  // wide steps add the lane themselves
     for (uint32_t it = blockIdx.x; it < L.nitems; it += gridDim.x) {
         const ItemInfo I = find_item(L, it);
         const Q8Job &J = job_at(L, I.job);
@@ -1254,11 +1306,21 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
                 const uint32_t ent = tsm[k];
                 const uint32_t f = ent >> 8, sym = ent & 0xFF;
                 const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
-                for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
+                for (uint32_t q = a; q < e; q++) {
+                    if constexpr (Cons::kWideLut)
+                        reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(f | (sym << 16), q - cum);
+                    else
+                        lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
+                }
                 cum += f;
             }
             if (cum < (uint32_t)qhi) {
-                for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) lut[q * 32 + lane] = 1u;
+                for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) {
+                    if constexpr (Cons::kWideLut)
+                        reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(1u, 0u);
+                    else
+                        lut[q * 32 + lane] = 1u;
+                }
                 atomicOr(L.status, MV_DEV_BAD_TABLE);
             }
             fence_proxy_async_smem();  // the table staging may share memory with later bulk copies
@@ -1364,9 +1426,10 @@ __global__ void q8s_scale_atomic_y(const Q8Job *jobs, int njobs, int batch) {
 
 namespace {
 
-size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage, size_t extra, size_t tbl_alias) {
+size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage, size_t extra, size_t tbl_alias,
+                bool wide_lut) {
     const size_t tbl = (size_t)tbl_stage * 2 <= tbl_alias ? 0 : (size_t)tbl_stage * 2;
-    return 256 * 32 * 4 + extra + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 +
+    return (size_t)256 * 32 * (wide_lut ? 8 : 4) + extra + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 +
            (size_t)W * DEPTH * 8 + 36 * 4 + (size_t)W * DEPTH * ILP * 4 + tbl;
 }
 
@@ -1394,7 +1457,7 @@ mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t 
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch: consumer region of %zu B breaks 16-byte alignment",
                     Cons::extra_bytes(W));
     const size_t smem = q8s_smem(Cons::kRedNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage, Cons::extra_bytes(W),
-                                 Cons::tbl_alias_bytes(W));
+                                 Cons::tbl_alias_bytes(W), Cons::kWideLut);
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch needs %zu B of shared memory (max %d)", smem,
                     max_smem_optin());
