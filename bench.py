@@ -696,7 +696,7 @@ def run_ours(args):
                          "algorithmic_bytes": alg, "peak_kind": peak_kind,
                          "kernel": "q8s_kernel<1,ILP,DEPTH> (mv_q8_stack_matvec)",
                          "note": "algorithmic bytes = compressed streams + tables + offsets + x + int32 y"},
-            "gpu_launches": args.steps * 3,
+            "gpu_launches": args.steps * S.launches_per_run,
             "clocks": sampler.summary(),
             "e2e": {"value": world * step_bytes / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

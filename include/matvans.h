@@ -151,9 +151,9 @@ mv_status mv_requant_absmax(const int32_t *y_dev, int n, int8_t *out8_dev, float
                             uint32_t *absmax_scratch_dev, void *stream);
 
 /* Allocation-free variant of mv_requant_absmax.  No counterpart in the
- * reference.  For callers that cannot allocate device memory: code enqueued
- * during CUDA graph capture, plugins whose host framework owns the allocator,
- * latency-critical paths that cannot afford cudaMalloc's implicit
+ * reference.  For callers that cannot allocate device memory: plugins whose
+ * host framework owns the allocator (and may hold all free memory in its
+ * pool), latency-critical paths that cannot afford cudaMalloc's implicit
  * synchronisation.  Same inputs, outputs and results as mv_requant_absmax,
  * but the reduction scratch is a 16 KiB array compiled into the library
  * (held on every GPU that loads it, until exit), so it calls no allocating
@@ -254,6 +254,7 @@ typedef struct mv_q8_stack_info {
     int32_t max_blk_rows;     /* shared-memory sizing over all jobs */
     uint32_t tbl_stripe_max;
     int32_t warps, ilp, depth;
+    int32_t atomic_jobs;      /* jobs whose rows span several work items (outputs zeroed, accumulated, scaled) */
 } mv_q8_stack_info;
 
 /* Plans a batched launch on the host: fills ngroups/atomic/item0 of every
@@ -265,9 +266,10 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
 /* Every job of a (device-resident, planned) job table in ONE persistent
  * launch: CTAs walk the (matrix, stripe, segment-group) work items of all
  * matrices, so uneven shapes share the GPU without per-matrix tails.  batch
- * 1..16.  Launches three kernels (zero atomically-accumulated outputs, the
- * persistent decode, scale them); capturable in a CUDA graph once the
- * device status word exists (any earlier call creates it). */
+ * 1..16.  Launches the persistent decode, plus a kernel before it that zeroes
+ * and one after it that scales the outputs of atomically-accumulated jobs
+ * when the plan has any (info->atomic_jobs > 0); capturable in a CUDA graph
+ * once the device status word exists (any earlier call creates it). */
 mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info,
                              int batch, const mv_q8_tuning *tuning, void *stream);
 

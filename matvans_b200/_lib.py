@@ -61,7 +61,8 @@ class Q8Job(ctypes.Structure):
 class Q8StackInfo(ctypes.Structure):
     """struct mv_q8_stack_info."""
     _fields_ = [("nitems", ctypes.c_uint32), ("max_blk_rows", ctypes.c_int32), ("tbl_stripe_max", ctypes.c_uint32),
-                ("warps", ctypes.c_int32), ("ilp", ctypes.c_int32), ("depth", ctypes.c_int32)]
+                ("warps", ctypes.c_int32), ("ilp", ctypes.c_int32), ("depth", ctypes.c_int32),
+                ("atomic_jobs", ctypes.c_int32)]
 
 
 _LIB = None

@@ -755,11 +755,11 @@ struct MmaCons {
             const int qc = 8 * p;
             if (qc + 8 <= nq) {
 #pragma unroll
-                for (int j = 0; j < 8; j++) w[j] = q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P);
+                for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P);
             } else {
 #pragma unroll
                 for (int j = 0; j < 8; j++)
-                    w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
+                    w[j] = (qc + j < nq) ? q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P) : 0u;
             }
             // the previous pair of MMAs is done with the A tile (and, at a window start, with the x tile)
             wait_mma(L);
@@ -791,11 +791,11 @@ struct MmaCons {
                 const int qc2 = qc + 8;
                 if (qc2 + 8 <= nq) {
 #pragma unroll
-                    for (int j = 0; j < 8; j++) w[j] = q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P);
+                    for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 8; j++)
-                        w[j] = (qc2 + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, L.lut_stride, P) : 0u;
+                        w[j] = (qc2 + j < nq) ? q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P) : 0u;
                 }
                 tmem_st_32x32b_x8_nowait(st_addr + 8u, w);
             }
@@ -855,15 +855,17 @@ __device__ __forceinline__ void i8x4_to_bf16x4(uint32_t wq, uint32_t &lo, uint32
 }
 
 // Decode one 8-quad piece of the lane's row (zeros past nq).
+template <bool kWide>
 __device__ __forceinline__ void decode_piece(int qc, int nq, uint32_t &lo, uint32_t &hi, uint32_t &k, uint32_t kend,
-                                             const uint32_t *sb, const uint32_t *lut_l, uint32_t stride, uint32_t &P,
-                                             uint32_t (&w)[8]) {
+                                             const uint32_t *sb, const uint32_t *lut_l, uint32_t stride, int lane,
+                                             uint32_t &P, uint32_t (&w)[8]) {
     if (qc + 8 <= nq) {
 #pragma unroll
-        for (int j = 0; j < 8; j++) w[j] = q8_step(lo, hi, k, kend, sb, lut_l, stride, P);
+        for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWide>(lo, hi, k, kend, sb, lut_l, stride, lane, P);
     } else {
 #pragma unroll
-        for (int j = 0; j < 8; j++) w[j] = (qc + j < nq) ? q8_step(lo, hi, k, kend, sb, lut_l, stride, P) : 0u;
+        for (int j = 0; j < 8; j++)
+            w[j] = (qc + j < nq) ? q8_step_t<kWide>(lo, hi, k, kend, sb, lut_l, stride, lane, P) : 0u;
     }
 }
 
@@ -961,7 +963,7 @@ struct FwdMma {
         const uint32_t kend = rows_now[0] * 32 + lane;
         for (int p = 0; p < npieces; p++) {
             uint32_t w[8];
-            decode_piece(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, P, w);
+            decode_piece<kWideLut>(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P, w);
             uint32_t a[16];
 #pragma unroll
             for (int j = 0; j < 8; j++) i8x4_to_bf16x4(w[j], a[2 * j], a[2 * j + 1]);
@@ -1153,7 +1155,7 @@ struct BwdMma {
                               (uint32_t)(lane & 7) * 16u;
         for (int p = 0; p < npieces; p++) {
             uint32_t w[8];
-            decode_piece(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, P, w);
+            decode_piece<kWideLut>(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P, w);
             uint32_t a[16];
 #pragma unroll
             for (int j = 0; j < 8; j++) i8x4_to_bf16x4(w[j], a[2 * j], a[2 * j + 1]);
@@ -1725,6 +1727,8 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
         info->tbl_stripe_max = std::max(info->tbl_stripe_max, m.tbl_stripe_max);
     }
     info->nitems = item;
+    info->atomic_jobs = 0;
+    for (int j = 0; j < njobs; j++) info->atomic_jobs += jobs[j].atomic ? 1 : 0;
     info->warps = t.warps;
     info->ilp = t.ilp;
     info->depth = t.depth;
@@ -1800,16 +1804,20 @@ mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_s
     L.tbl_stage = (int)((info->tbl_stripe_max + 7) & ~7u);
     L.lut_stride = 32;
     dim3 zg(64, std::min(njobs, 1024));
-    mv::q8s_zero_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
-    MV_CUDA_TRY(cudaGetLastError(), "q8s_zero_atomic_y launch");
+    if (info->atomic_jobs > 0) {
+        mv::q8s_zero_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
+        MV_CUDA_TRY(cudaGetLastError(), "q8s_zero_atomic_y launch");
+    }
     if (mv::nv_round(batch) >= 8 && t.engine == MV_ENGINE_AUTO) {  // the tensor-core consumer reads x tiles
         mv::q8s_build_x_tiles<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
         MV_CUDA_TRY(cudaGetLastError(), "q8s_build_x_tiles launch");
     }
     rc = mv::launch_q8s(L, mv::nv_round(batch), t, st);
     if (rc) return rc;
-    mv::q8s_scale_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
-    MV_CUDA_TRY(cudaGetLastError(), "q8s_scale_atomic_y launch");
+    if (info->atomic_jobs > 0) {
+        mv::q8s_scale_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);
+        MV_CUDA_TRY(cudaGetLastError(), "q8s_scale_atomic_y launch");
+    }
     return MV_OK;
 }
 

@@ -1,11 +1,11 @@
 // mv_requant_absmax_noalloc: the absmax requantisation of mv_requant_absmax
 // for callers that cannot allocate device memory.
 //
-// Who cannot allocate: code that enqueues work while a CUDA graph is being
-// captured (cudaMalloc is not a capturable operation), plugins embedded in a
-// host framework that owns the device allocator and forbids allocations behind
-// its back, and latency-critical paths where the implicit device
-// synchronisation of cudaMalloc/cudaFree is not acceptable.  mv_requant_absmax
+// Who cannot allocate: plugins embedded in a host framework that owns the
+// device allocator and forbids allocations behind its back (its pool may hold
+// all free memory, so a cudaMalloc would fail or starve it), and
+// latency-critical paths where the implicit device synchronisation of
+// cudaMalloc/cudaFree is not acceptable.  mv_requant_absmax
 // needs a caller-owned scratch word for its reduction; this variant keeps its
 // scratch in a fixed array compiled into the library instead, and calls no
 // allocating routine at all (not cudaMalloc, not cudaFree, no allocating

@@ -274,8 +274,10 @@ class Q8Stack:
                     for M in self.matrices] if scales is not None else None
         n = len(self.matrices)
         jobs = (Q8Job * n)()
-        # 8..16 vectors on the tensor cores: x is laid out in tiles first (device scratch per matrix)
-        use_tiles = self.batch >= 8 and self.tuning.engine == 0
+        # 5..16 vectors (rounded up to 8 or 16) run on the tensor cores: x is laid out in tiles first
+        # (device scratch per matrix)
+        self._tiled = self.batch >= 5 and self.tuning.engine == 0
+        use_tiles = self._tiled
         self.x_tiles = []
         for i, M in enumerate(self.matrices):
             x = self.xs[i]
@@ -301,6 +303,12 @@ class Q8Stack:
     @property
     def nitems(self):
         return self.info.nitems
+
+    @property
+    def launches_per_run(self):
+        """Kernels one run() launches: the persistent decode, the x-tile layout pass when the tensor-core
+        consumer reads x tiles, and the zero/scale passes when any job accumulates atomically."""
+        return 1 + (1 if self._tiled else 0) + (2 if self.info.atomic_jobs else 0)
 
     def run(self):
         check(lib().mv_q8_stack_matvec(_p(self.jobs_dev), len(self.matrices), ctypes.byref(self.info), self.batch,

@@ -1,8 +1,8 @@
 """The allocation-free requantisation entry point against the scratch-taking one.
 
 mv_requant_absmax_noalloc exists for callers that cannot allocate device memory
-(for example code enqueued while a CUDA graph is being captured, or a plugin
-whose host framework owns the allocator).  It must give exactly the results of
+(for example a plugin whose host framework owns the allocator, or a latency path
+that cannot take cudaMalloc's implicit synchronisation).  It must give exactly the results of
 mv_requant_absmax, which takes caller-owned scratch, on consecutive calls that
 reuse its static scratch array.  Called through the C ABI.
 """
