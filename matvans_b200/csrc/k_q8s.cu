@@ -28,9 +28,9 @@
 // | r << 24 with f the symbol's frequency, r = q - cum < f <= 255):
 //   refill:   if (hi == 0) { hi = lo; lo = next word }
 //   lookups:  e_i = table[byte i of lo]
-//   update:   t2 = r2 + f2*r3, t1 = r1 + f1*t2, f0*f1, f2*f3 (dp2a: 16-bit x
-//             8-bit dot products read f straight from the entries), t0 =
-//             r0 + f0*t1, P = (f0 f1)(f2 f3), (hi:lo) = hi*P + t0 (one
+//   update:   u01 = r0 + f0*r1, t2 = r2 + f2*r3, f0*f1, f2*f3 (dp2a: 16-bit
+//             x 8-bit dot products read f straight from the entries), t0 =
+//             u01 + (f0 f1) t2, P = (f0 f1)(f2 f3), (hi:lo) = hi*P + t0 (one
 //             32x32->64 IMAD)
 #include <algorithm>
 #include <cstdio>
@@ -211,12 +211,12 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
     // entry = f | sym << 16 | r << 24 (byte 1 zero, so the low half-word is exactly f)
     const uint32_t r0 = __umulhi(e0, 256u), r1 = __umulhi(e1, 256u);
     const uint32_t r2 = e2 >> 24, r3 = e3 >> 24;
+    const uint32_t u01 = __dp2a_lo(r1, e0, r0);     // r0 + f0*r1
     const uint32_t t2 = __dp2a_lo(r3, e2, r2);      // r2 + f2*r3
-    const uint32_t t1 = __dp2a_lo(t2, e1, r1);      // r1 + f1*t2  (t2 < 2^16)
     const uint32_t p01 = __dp2a_lo(e1, e0, 0u);     // f1*f0 + (sym1 | r1 << 8) * 0
     const uint32_t p23 = __dp2a_lo(e3, e2, 0u);     // f3*f2
     P = p01 * p23;
-    const uint32_t t0 = r0 + (e0 & 0xFFu) * t1;
+    const uint32_t t0 = u01 + p01 * t2;             // r0 + f0 r1 + f0 f1 (r2 + f2 r3) < P
     const unsigned long long s = (unsigned long long)hi * P + t0;
     lo = (uint32_t)s;
     hi = (uint32_t)(s >> 32);
@@ -238,12 +238,12 @@ __device__ __forceinline__ uint32_t q8_step_wide(uint32_t &lo, uint32_t &hi, uin
     const uint2 e1 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5514));
     const uint2 e2 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5524));
     const uint2 e3 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5534));
-    const uint32_t t2 = __dp2a_lo(e3.y, e2.x, e2.y);  // r2 + f2*r3
-    const uint32_t t1 = __dp2a_lo(t2, e1.x, e1.y);    // r1 + f1*t2  (t2 < 2^16)
-    const uint32_t p01 = __dp2a_lo(e1.x, e0.x, 0u);   // f1*f0 + sym1*0
-    const uint32_t p23 = __dp2a_lo(e3.x, e2.x, 0u);   // f3*f2
+    const uint32_t u01 = __dp2a_lo(e1.y, e0.x, e0.y);  // r0 + f0*r1
+    const uint32_t t2 = __dp2a_lo(e3.y, e2.x, e2.y);   // r2 + f2*r3
+    const uint32_t p01 = __dp2a_lo(e1.x, e0.x, 0u);    // f1*f0 + sym1*0
+    const uint32_t p23 = __dp2a_lo(e3.x, e2.x, 0u);    // f3*f2
     P = p01 * p23;
-    const uint32_t t0 = e0.y + (e0.x & 0xFFu) * t1;
+    const uint32_t t0 = u01 + p01 * t2;                // r0 + f0 r1 + f0 f1 (r2 + f2 r3) < P
     const unsigned long long s = (unsigned long long)hi * P + t0;
     lo = (uint32_t)s;
     hi = (uint32_t)(s >> 32);
