@@ -36,9 +36,9 @@ SIGMAS = [4.0, 2.0]
 METRIC = "us/matvec & int8-equiv GB/s vs dense dp4a int8 on B200, bit-exact int32 output"
 UNIT = "GB/s"
 L2_BYTES = 126 * 2 ** 20
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the step's kernel (q8s_kernel, 4 warps, ilp 1),
-# from an ncu --set full capture of `bench.py --profile --tuning 4,1,1,0,0,0`
-STEP_DRAM_BYTES = 215.6e6
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the step's kernel (q8s_kernel, 8 warps, ilp 1),
+# from an ncu --set full capture of `bench.py --profile --tuning 8,1,1,0,0,0`
+STEP_DRAM_BYTES = 215.3e6
 
 
 def gen_matrix(shape, sigma, seed):

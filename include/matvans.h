@@ -202,7 +202,8 @@ mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int3
 /* Launch parameters of the persistent Q8 kernel (0 = library default).
  *   warps        warps per CTA (1..8, default 8; up to 16 when the tensor-core
  *                engine runs, i.e. 8..16 vectors with engine 0)
- *   ilp          independent segments decoded per warp (1 or 2, default 2)
+ *   ilp          independent segments decoded per warp (1 or 2, default 2;
+ *                1 for the float form)
  *   depth        shared-memory stream buffers per warp (1 or 2, default 1):
  *                2 keeps the next work item's bulk copies in flight
  *   ctas_per_sm  cap on resident CTAs per SM (default: occupancy limit)

@@ -442,7 +442,7 @@ struct BwdCons {
     static constexpr int kMinCtas = 1;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
-    static constexpr bool kWideLut = true;
+    static constexpr bool kWideLut = false;  // its shuffle reduction already loads the shared-memory pipe
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
@@ -1643,7 +1643,8 @@ mv_status q8f_run(const mv_q8_view *m, int mode, const uint16_t *in, int batch, 
     mv_status rc;
     uint32_t *status = device_status_word(&rc);
     if (rc) return rc;
-    const mv_q8_tuning t = resolve(tuning);
+    mv_q8_tuning t = resolve(tuning);
+    if (!tuning || (tuning->ilp != 1 && tuning->ilp != 2)) t.ilp = 1;  // the float form's default
     const int in_len = mode == 1 ? m->cols : m->rows;   // elements per vector in
     const int out_len = mode == 1 ? m->rows : m->cols;  // elements per vector out
     if (mode == 2) MV_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)batch * out_len, st), "memset(dx)");
@@ -1694,6 +1695,7 @@ mv_status mv_q8_matvec_bf16(const mv_q8_view *m, const uint16_t *x_dev, int batc
         return mv::fail(MV_ERR_ARG, "mv_q8_matvec_bf16: needs cols %% 16 == 0, seg_quads %% 4 == 0, 16-byte aligned x");
     mv_q8_tuning t = mv::resolve(tuning);
     t.parts = 1;
+    if (!tuning || (tuning->ilp != 1 && tuning->ilp != 2)) t.ilp = 1;  // the float form's default
     return mv::q8f_run(m, 1, x_dev, batch, row_scales_dev, y_dev, &t, (cudaStream_t)stream);
 }
 
