@@ -268,7 +268,10 @@ class Q8Stack:
         self.tuning = tuning if isinstance(tuning, Q8Tuning) else Q8Tuning(*(tuning or (0, 0, 0, 0)))
         self.xs = xs if xs is not None else [torch.zeros((self.batch, M.cols), dtype=torch.int8, device=self.device)
                                              for M in self.matrices]
-        self.ys = [torch.empty((self.batch, M.rows), dtype=torch.int32, device=self.device) for M in self.matrices]
+        # outputs: views into one contiguous int32 buffer in job order (y_flat), so that one copy moves them all
+        sizes = [self.batch * M.rows for M in self.matrices]
+        self.y_flat = torch.empty(sum(sizes), dtype=torch.int32, device=self.device)
+        self.ys = [v.view(self.batch, M.rows) for v, M in zip(torch.split(self.y_flat, sizes), self.matrices)]
         self.scales = scales
         self.yss = [torch.empty((self.batch, M.rows), dtype=torch.float32, device=self.device)
                     for M in self.matrices] if scales is not None else None
@@ -341,7 +344,10 @@ class Q8Chain:
                                                           device=self.device)]
         self.xs += [torch.zeros((self.batch, M.cols), dtype=torch.int8, device=self.device)
                     for M in self.matrices[1:]]
-        self.ys = [torch.empty((self.batch, M.rows), dtype=torch.int32, device=self.device) for M in self.matrices]
+        # outputs: views into one contiguous int32 buffer in job order (y_flat), so that one copy moves them all
+        sizes = [self.batch * M.rows for M in self.matrices]
+        self.y_flat = torch.empty(sum(sizes), dtype=torch.int32, device=self.device)
+        self.ys = [v.view(self.batch, M.rows) for v, M in zip(torch.split(self.y_flat, sizes), self.matrices)]
         self.out8 = torch.empty((self.batch, self.matrices[-1].rows), dtype=torch.int8, device=self.device)
         n = len(self.matrices)
         jobs = (Q8Job * n)()
