@@ -9,9 +9,14 @@
 // format, so this kernel keeps one warp per row and reproduces it exactly.
 // What changes on B200:
 //   * the three 32-entry packed tables are expanded once per CTA into a
-//     128-quantile x 32-lane shared table (entry (q,l) at word q*32 + l), so
-//     the four lookups of a quad are four conflict-free loads instead of
-//     twelve warp shuffles (ans-warp-rows-kernel.cu:147-189);
+//     128-quantile x 32-lane shared table of 8-byte entries {p | sym << 16,
+//     q - cum} at byte q*256 + l*8, so the four lookups of a quad are four
+//     conflict-free loads instead of twelve warp shuffles
+//     (ans-warp-rows-kernel.cu:147-189), each address is one shift and one
+//     three-input logic op of the state, and q - cum arrives as a clean word;
+//   * the state update forms the reference's r0 + p0 r1 + p0p1 r2 + p0p1p2 r3
+//     (ans-warp-rows-kernel.cu:198-202) as (r0 + p0 r1) + (p0 p1)(r2 + p2 r3)
+//     with 16x8-bit dot products: the same integer, fewer instructions;
 //   * the warp cache advances lazily: a block is loaded only when a lane
 //     actually consumes one of its words (the reference also reloads when the
 //     cursor lands exactly on a block boundary, which can read past the row);
@@ -48,8 +53,8 @@ struct AwrLaunch {
 template <int NV, bool REQUANT, bool STRIPES>
 __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t *lut = reinterpret_cast<uint32_t *>(smem);  // 128 * 32 words
-    uint32_t *xs = lut + 128 * 32;                       // [cols/4][NV]
+    uint2 *lut = reinterpret_cast<uint2 *>(smem);        // 128 * 32 entries of 8 bytes
+    uint32_t *xs = reinterpret_cast<uint32_t *>(lut + 128 * 32);  // [cols/4][NV]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
     const int nq = L.cols >> 2;
 
@@ -59,7 +64,7 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
         const uint32_t c = (__ldg(L.cum + (q >> 2)) >> sh) & 0xFF;
         const uint32_t p = (__ldg(L.prob + (q >> 2)) >> sh) & 0xFF;
         if (c > q || p == 0) atomicOr(L.status, MV_DEV_BAD_TABLE);
-        lut[i] = sym | (p << 8) | (((q - c) & 0xFFFF) << 16);
+        lut[i] = make_uint2(p | (sym << 16), (q - c) & 0xFFFFu);
     }
     const bool xal = (reinterpret_cast<uintptr_t>(L.x) & 3) == 0;
     for (int i = threadIdx.x; i < nq * NV; i += blockDim.x) {
@@ -75,7 +80,8 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
     __syncthreads();
 
     const uint32_t lt_mask = (1u << lane) - 1u;
-    const uint32_t *lut_l = lut + lane;
+    const unsigned char *lut_b = reinterpret_cast<const unsigned char *>(lut);
+    const uint32_t lane8 = (uint32_t)lane << 3;
     const bool bounded = L.n_u4 != 0;
 
     const int units = STRIPES ? L.rows / 32 : L.rows;  // warps' work units: rows or 32-row stripes
@@ -135,17 +141,18 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
                 wcc = (wcc + num) & 127;
             }
             const uint32_t lo = (uint32_t)state;
-            const uint32_t e0 = lut_l[(lo & 0x7Fu) << 5];
-            const uint32_t e1 = lut_l[((lo >> 7) & 0x7Fu) << 5];
-            const uint32_t e2 = lut_l[((lo >> 14) & 0x7Fu) << 5];
-            const uint32_t e3 = lut_l[((lo >> 21) & 0x7Fu) << 5];
-            const uint32_t p0 = __byte_perm(e0, 0, 0x4441), p1 = __byte_perm(e1, 0, 0x4441);
-            const uint32_t p2 = __byte_perm(e2, 0, 0x4441), p3 = __byte_perm(e3, 0, 0x4441);
-            const uint32_t p01 = p0 * p1, p012 = p01 * p2, p0123 = p012 * p3;
-            const uint32_t ns = (e0 >> 16) + p0 * (e1 >> 16) + p01 * (e2 >> 16) + p012 * (e3 >> 16);
-            state = (state >> 28) * (unsigned long long)p0123 + ns;
+            // quantile k (bits 7k..7k+6) moved to bits 8..14, the lane's byte offset in bits 0..7
+            const uint2 e0 = *reinterpret_cast<const uint2 *>(lut_b + (((lo << 8) & 0x7F00u) | lane8));
+            const uint2 e1 = *reinterpret_cast<const uint2 *>(lut_b + (((lo << 1) & 0x7F00u) | lane8));
+            const uint2 e2 = *reinterpret_cast<const uint2 *>(lut_b + (((lo >> 6) & 0x7F00u) | lane8));
+            const uint2 e3 = *reinterpret_cast<const uint2 *>(lut_b + (((lo >> 13) & 0x7F00u) | lane8));
+            const uint32_t u01 = __dp2a_lo(e1.y, e0.x, e0.y);  // r0 + p0 r1
+            const uint32_t t2 = __dp2a_lo(e3.y, e2.x, e2.y);   // r2 + p2 r3
+            const uint32_t p01 = __dp2a_lo(e1.x, e0.x, 0u);    // p0 p1 (+ sym1 * 0)
+            const uint32_t p23 = __dp2a_lo(e3.x, e2.x, 0u);    // p2 p3
+            state = (state >> 28) * (unsigned long long)(p01 * p23) + (u01 + p01 * t2);
             const uint32_t wq =
-                __byte_perm(__byte_perm(e0, e1, 0x0040), __byte_perm(e2, e3, 0x0040), 0x5410);
+                __byte_perm(__byte_perm(e0.x, e1.x, 0x0062), __byte_perm(e2.x, e3.x, 0x0062), 0x5410);
             const uint32_t *xq = xs + (STRIPES ? j : j + lane) * NV;  // stripes: one x quad for all lanes
 #pragma unroll
             for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wq, (int)xq[v], acc[v]);
@@ -195,7 +202,7 @@ mv_status launch_awr(const AwrLaunch &L, cudaStream_t st) {
     // stripes: few work units (rows / 32, each decoded start to end by one warp), so one-warp CTAs spread
     // them over all SMs
     const int W = STRIPES ? 1 : 8;
-    const size_t smem = 128 * 32 * 4 + (size_t)(L.cols / 4) * NV * 4;
+    const size_t smem = 128 * 32 * 8 + (size_t)(L.cols / 4) * NV * 4;
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "AWR: %d columns x %d vectors exceed shared memory", L.cols, NV);
     auto kern = awr_kernel<NV, REQUANT, STRIPES>;
