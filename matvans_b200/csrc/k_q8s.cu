@@ -1304,6 +1304,36 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
             const uint32_t o0 = toff_s[t], o1 = max(toff_s[t + 1], o0);
             const int qlo = (256 * warp) / W, qhi = (256 * (warp + 1)) / W;
             uint32_t cum = 0;
+            if (Cons::kWideLut && !m.local) {
+                // one table for every row: lane j finds the entry of quantile qlo + j (the lanes walk the symbols
+                // together, without divergence) and writes it to all 32 lane columns, rotating the column so
+                // that a half-warp's stores hit distinct banks
+                uint2 *lut2 = reinterpret_cast<uint2 *>(lut);
+                bool bad = false;
+                for (uint32_t q0 = (uint32_t)qlo; q0 < (uint32_t)qhi; q0 += 32) {
+                    const uint32_t q = q0 + lane, qend = min(q0 + 32, (uint32_t)qhi);
+                    uint32_t c = 0, ent_q = 0, cum_q = 0;
+                    bool found = false;
+                    for (uint32_t k = o0; k < o1 && c < qend; k++) {
+                        const uint32_t ent = tsm[k], f = ent >> 8;
+                        if (!found && q < c + f) {  // q >= c: no earlier symbol contains q
+                            ent_q = ent;
+                            cum_q = c;
+                            found = true;
+                        }
+                        c += f;
+                    }
+                    if (q < qend) {
+                        bad |= !found;
+                        const uint2 v = found ? make_uint2((ent_q >> 8) | ((ent_q & 0xFFu) << 16), q - cum_q)
+                                              : make_uint2(1u, 0u);
+#pragma unroll 8
+                        for (uint32_t i = 0; i < 32; i++) lut2[q * 32 + ((lane + i) & 31)] = v;
+                    }
+                }
+                if (bad) atomicOr(L.status, MV_DEV_BAD_TABLE);
+                cum = (uint32_t)qhi;  // done: the per-lane loops below do nothing
+            }
             for (uint32_t k = o0; k < o1 && cum < (uint32_t)qhi; k++) {
                 const uint32_t ent = tsm[k];
                 const uint32_t f = ent >> 8, sym = ent & 0xFF;
