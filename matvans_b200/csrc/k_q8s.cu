@@ -1334,7 +1334,18 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
                 if (bad) atomicOr(L.status, MV_DEV_BAD_TABLE);
                 cum = (uint32_t)qhi;  // done: the per-lane loops below do nothing
             }
-            for (uint32_t k = o0; k < o1 && cum < (uint32_t)qhi; k++) {
+            uint32_t k = o0;
+            if (Cons::kWideLut && cum < (uint32_t)qlo) {
+                // symbols that end at or before qlo: one load, shift and add each (measured: 0.8 % faster for
+                // the CUDA-core consumers, 0.6 % slower for the tensor-core one, which keeps the plain loop)
+                uint32_t f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+                while (k < o1 && cum + f <= (uint32_t)qlo) {
+                    cum += f;
+                    k++;
+                    f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+                }
+            }
+            for (; k < o1 && cum < (uint32_t)qhi; k++) {
                 const uint32_t ent = tsm[k];
                 const uint32_t f = ent >> 8, sym = ent & 0xFF;
                 const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
