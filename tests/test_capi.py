@@ -31,3 +31,27 @@ def test_version_and_error_string():
     rc = L.mv_awr_encode(None, 0, 0, 0, ctypes.byref(ctypes.c_void_p()))
     assert rc == 1
     assert b"bad arguments" in L.mv_last_error()
+
+
+def test_stack_plan_reports_atomic_jobs():
+    """The stack plan counts the jobs whose rows span several work items (parts > 1 and more than one
+    segment): only then does the launch add its zero and scale passes.  Host only."""
+    from matvans_b200._lib import Q8Job, Q8StackInfo, Q8Tuning
+    L = _lib.lib()
+    jobs = (Q8Job * 3)()
+    for i, (r, c) in enumerate([(64, 512), (32, 64), (96, 1024)]):
+        jobs[i].m.rows, jobs[i].m.cols = r, c
+        jobs[i].m.seg_quads = 16
+        jobs[i].m.nseg = -(-(c // 4) // 16)
+        jobs[i].m.local = 1
+        jobs[i].m.max_blk_rows = 4
+    info = Q8StackInfo()
+    assert L.mv_q8_stack_plan(jobs, 3, ctypes.byref(Q8Tuning(8, 1, 1, 0, 0, 0)), ctypes.byref(info)) == 0
+    assert info.atomic_jobs == 0 and all(jobs[i].atomic == 0 for i in range(3))
+    assert info.nitems == 2 + 1 + 3
+    # parts = 4: every job with more than one segment is split (and accumulates atomically); the
+    # 64-column job has a single segment and stays whole
+    assert L.mv_q8_stack_plan(jobs, 3, ctypes.byref(Q8Tuning(8, 1, 1, 0, 4, 0)), ctypes.byref(info)) == 0
+    assert [jobs[i].ngroups for i in range(3)] == [4, 1, 4]
+    assert info.atomic_jobs == 2 and [jobs[i].atomic for i in range(3)] == [1, 0, 1]
+    assert info.nitems == 2 * 4 + 1 + 3 * 4
