@@ -1349,11 +1349,13 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
                 const uint32_t ent = tsm[k];
                 const uint32_t f = ent >> 8, sym = ent & 0xFF;
                 const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
-                for (uint32_t q = a; q < e; q++) {
-                    if constexpr (Cons::kWideLut)
+                if constexpr (Cons::kWideLut) {
+                    for (uint32_t q = a; q < e; q++)
                         reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(f | (sym << 16), q - cum);
-                    else
-                        lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
+                } else {
+                    // unrolled: measured 1 % faster for the tensor-core consumer (0.4 % slower for the wide table)
+#pragma unroll 4
+                    for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
                 }
                 cum += f;
             }
