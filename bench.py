@@ -125,33 +125,47 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ CPU legs
 
+def headline_config():
+    """The workload both arms measure (the reference arm decodes the same 12 matvecs)."""
+    return {"workload": "7B-layer single-vector int8 matvecs: W_q 4096x4096, 11008x4096 and 4096x11008 at sigma 4 "
+                        "and 2, each once as a global-CDF and once as a per-row-CDF matvec (12 matvecs per step), "
+                        "B=1, seeded synthetic int8 weights and x",
+            "batch": 1, "matvecs_per_step": 2 * len(SHAPES) * len(SIGMAS), "seed": 20251203,
+            "l2": "inputs larger than L2: the 12 matrices' compressed streams (about 200 MB) exceed the 126 MiB "
+                  "L2 and each is read once per step"}
+
+
+def cpu_encode_all(mats):
+    """Each matrix in the reference's ans-warp-rows layout, encoded by the oracle's restatement of the reference
+    encoder (buffered/encoder.py:271-470; byte-identical on the reference-made fixtures), so that the CPU legs
+    load no product code."""
+    import oracle
+    out = []
+    for m in mats:
+        comp, offs, p, c, pr = oracle.awr_encode(m["W"])
+        out.append(dict(shape=m["shape"], sigma=m["sigma"], compressed=comp, offsets=offs, ppf=p, cum=c, prob=pr))
+    return out
+
+
 def cpu_reference_pass(awr_mats, x_by_cols, nthreads):
-    """One pass of the oracle's AWR decode + matvec over the AWR-encoded matrices."""
+    """One pass of the reference algorithm over the 12 matvecs of a step: the reference has one layout (a global
+    CDF per matrix), so each matrix is decoded for its global-CDF and for its per-row-CDF matvec.  Decode + int8
+    dot products by the oracle's C restatement of buffered/ans-warp-rows-kernel.cu:20-210."""
     import oracle
     nbytes = 0
     for m in awr_mats:
         rows, cols = m["shape"]
-        y = oracle.awr_matvec(m["compressed"], m["offsets"], rows, cols, m["ppf"], m["cum"], m["prob"],
-                              x_by_cols[cols], nthreads=nthreads)
-        assert y.shape == (rows,)
-        nbytes += int8_equiv_bytes(rows, cols)
+        for _ in range(2):
+            y = oracle.awr_matvec(m["compressed"], m["offsets"], rows, cols, m["ppf"], m["cum"], m["prob"],
+                                  x_by_cols[cols], nthreads=nthreads)
+            assert y.shape == (rows,)
+            nbytes += int8_equiv_bytes(rows, cols)
     return nbytes
-
-
-def awr_encode_all(mats):
-    from matvans_b200 import codec
-    out = []
-    for m in mats:
-        comp, offs, mn, cdf = codec.compress_ans_warp_rows(m["W"])
-        p, pc, pp = codec.decoder_model_from_128bit_encoder_model(mn, cdf)
-        out.append(dict(shape=m["shape"], sigma=m["sigma"], compressed=comp, offsets=offs,
-                        ppf=codec.pack_4bytes(p), cum=codec.pack_4bytes(pc), prob=codec.pack_4bytes(pp)))
-    return out
 
 
 def cpu_baseline(mats, x_by_cols, budget_s=8.0):
     nthreads = os.cpu_count() or 1
-    awr = awr_encode_all(mats)
+    awr = cpu_encode_all(mats)
     t0 = time.perf_counter()
     nbytes, passes = 0, 0
     while True:
@@ -161,19 +175,29 @@ def cpu_baseline(mats, x_by_cols, budget_s=8.0):
             break
     dt = time.perf_counter() - t0
     return {"value": nbytes / dt / 1e9, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": f"{passes} pass(es) over the 6 ans-warp-rows encodings (3 shapes x sigma 4,2) of the "
-                      f"workload, oracle C decode+matvec, {nthreads} threads, {dt:.1f} s"}
+            "sample": f"{passes} pass(es) over the step's 12 matvecs (the 6 matrices in the reference's "
+                      f"ans-warp-rows layout, each decoded twice), oracle C decode+matvec, {nthreads} threads, "
+                      f"{dt:.1f} s"}
 
 
 def run_reference(args):
+    """The reference's CPU implementation of the path on this host's cores: no product library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     mats = workload()
     rng = np.random.default_rng(7)
     x_by_cols = {c: rng.integers(-127, 128, size=c).astype(np.int8) for c in {s[1] for s in SHAPES}}
-    awr = awr_encode_all(mats)
+    awr = cpu_encode_all(mats)
     nthreads = os.cpu_count() or 1
+    # gate: every decoded product equals the int64 matvec of the original matrix
+    import oracle
+    for m, a in zip(mats, awr):
+        rows, cols = m["shape"]
+        y = oracle.awr_matvec(a["compressed"], a["offsets"], rows, cols, a["ppf"], a["cum"], a["prob"],
+                              x_by_cols[cols], nthreads=nthreads)
+        if not np.array_equal(y, oracle.matvec_i8(m["W"], x_by_cols[cols])):
+            raise SystemExit("bench --impl reference: decoded product is not exact")
     for _ in range(args.warmup):
         cpu_reference_pass(awr, x_by_cols, nthreads)
     t0 = time.perf_counter()
@@ -185,13 +209,13 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": "7B-layer single-vector matvecs, ans-warp-rows layout (the reference's only "
-                                   "CPU-decodable layout): W_q 4096x4096, 11008x4096, 4096x11008 at sigma 4 and 2, "
-                                   "global CDF, B=1", "batch": 1, "seed": 20251203},
+            "impl": "reference", "config": headline_config(),
+            "layout": "the reference's ans-warp-rows layout (one global CDF per matrix, its only layout), encoded by "
+                      "the oracle's restatement of buffered/encoder.py",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": f"each step one pass over the 6 matrices with the oracle's C restatement "
-                                       f"of the reference decoder, {nthreads} threads"},
+                             "sample": f"each step one pass over the 12 matvecs with the oracle's C restatement of "
+                                       f"the reference decoder (buffered/ans-warp-rows-kernel.cu), {nthreads} "
+                                       f"threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -679,14 +703,12 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-            "config": {"workload": "7B-layer single-vector matvecs (Q8-stripe layout): W_q 4096x4096, 11008x4096, "
-                                   "4096x11008 at sigma 4 and 2, each with a global and a per-row CDF; 12 matvecs "
-                                   "per step, B=1, seeded synthetic int8 weights and x",
-                       "batch": 1, "matvecs_per_step": len(entries), "seed": 20251203,
-                       "l2": f"working set {alg / 2**20:.0f} MiB > 126 MiB L2, each matrix read once per step",
-                       "timing": "CUDA graph of one step (one persistent launch over the 12 matrices), CUDA "
-                                 "events over K replays, max over ranks",
-                       "stack_tuning": list(stack_tuning), "stack_candidates_us": stack_cands},
+            "config": headline_config(),
+            "layout": "Q8-stripe layout: 6 matrices with one global table, 6 with per-row tables; working set "
+                      f"{alg / 2**20:.0f} MiB of compressed streams, tables and offsets",
+            "timing": "CUDA graph of one step (one persistent launch over the 12 matrices), CUDA events over K "
+                      "replays in windows, max over ranks; ms_per_step is the median window",
+            "stack_tuning": list(stack_tuning), "stack_candidates_us": stack_cands,
             "us_per_matvec": {k: round(v["us"], 3) for k, v in per.items()},
             "per_matrix": per,
             "dense_dp4a": dense, "cublas_sgemv_fp32": cublas, "ans_warp_rows_kernel": awr_t,

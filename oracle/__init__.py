@@ -51,7 +51,10 @@ def lib():
                                         ctypes.c_int, P, ctypes.c_int]
         L.orc_aws_decode.argtypes = [P, i64, P, i64, i64, P, P, P, P]
         L.orc_aws_matvec.argtypes = [P, i64, P, i64, i64, P, P, P, P, ctypes.c_int, P]
-        for f in ("orc_matvec_i8", "orc_awr_decode", "orc_wpr_decode", "orc_awr_matvec_mt",
+        L.orc_awr_encode.argtypes = [P, i64, i64, ctypes.POINTER(P), ctypes.POINTER(i64), P, P, P, P]
+        L.orc_free.argtypes = [P]
+        L.orc_free.restype = None
+        for f in ("orc_matvec_i8", "orc_awr_decode", "orc_wpr_decode", "orc_awr_matvec_mt", "orc_awr_encode",
                   "orc_wpr_matvec_mt", "orc_aws_decode", "orc_aws_matvec"):
             getattr(L, f).restype = ctypes.c_int
         _LIB = L
@@ -97,6 +100,24 @@ def awr_decode(compressed, offsets, rows, cols, ppf, ppf_cum, ppf_prob):
     _check(lib().orc_awr_decode(_p(comp), comp.size, _p(offs), rows, cols, *[_p(a) for a in t], _p(W)),
            "awr_decode")
     return W
+
+
+def awr_encode(W):
+    """The reference's compress_ans_warp_rows(W, 32) with its decoder tables (buffered/encoder.py:271-320,
+    394-470), restated in C: returns (compressed u32, warp_offsets u32[rows], ppf, ppf_cum, ppf_prob u32[32])."""
+    W = _c(W, np.int8)
+    rows, cols = W.shape
+    comp = ctypes.c_void_p()
+    n = ctypes.c_int64()
+    offs = np.empty(rows, np.uint32)
+    t = [np.empty(32, np.uint32) for _ in range(3)]
+    _check(lib().orc_awr_encode(_p(W), rows, cols, ctypes.byref(comp), ctypes.byref(n), _p(offs),
+                                *[_p(a) for a in t]), "awr_encode")
+    try:
+        out = np.ctypeslib.as_array(ctypes.cast(comp, ctypes.POINTER(ctypes.c_uint32)), shape=(n.value,)).copy()
+    finally:
+        lib().orc_free(comp)
+    return out, offs, t[0], t[1], t[2]
 
 
 def awr_matvec(compressed, offsets, rows, cols, ppf, ppf_cum, ppf_prob, x, nthreads=1):

@@ -374,3 +374,165 @@ int orc_wpr_matvec_mt(const uint16_t *payload, int64_t payload_size, const uint3
     jb.min_value = min_value; jb.cdf = cdf; jb.G = G; jb.ppf8 = ppf;
     return orc_run(&jb, nthreads);
 }
+
+/* ------------------------------------------------------------ AWR encoder */
+
+/*
+ * The reference's ans-warp-rows encoder, restated so that the CPU legs of the
+ * benchmark can build their inputs without the product library:
+ *   fit_128bit_encoder_model           buffered/encoder.py:271-306
+ *   DetachedAnsQuadCoder.encode        buffered/encoder.py:190-226
+ *   compress_ans_warp_rows(matrix, 32) buffered/encoder.py:394-461
+ *   decoder tables + pack_4bytes       buffered/encoder.py:309-320, 464-470
+ * Output is byte-identical to the reference encoder (tests/golden/awr_cases.npz).
+ * *comp_out is malloc'd (free with orc_free); offsets has `rows` entries (uint4
+ * units); ppf/cum/prob are u32[32] each.
+ */
+static int awr_fit(const int8_t *W, int64_t n, int *min_value, uint8_t *cdf, int *ncdf)
+{
+    int64_t hist[256];
+    memset(hist, 0, sizeof hist);
+    for (int64_t i = 0; i < n; i++) hist[(uint8_t)W[i] ^ 0x80]++;
+    int vals[256], nv = 0;
+    for (int v = 0; v < 256; v++)
+        if (hist[v]) vals[nv++] = v;
+    if (nv > 128) return ORC_ERR_MODEL;  /* encoder.py:303: at most 128 values */
+    /* pmf = max(1, round(float32(count) * 128 / numel)) in float32, half to even (encoder.py:278-280) */
+    uint32_t pmf[256];
+    const float numel = (float)n;
+    uint64_t sum = 0;
+    for (int i = 0; i < nv; i++) {
+        volatile float t = (float)hist[vals[i]] * 128.0f;
+        volatile float q = t / numel;
+        uint32_t u = (uint32_t)nearbyintf(q);
+        pmf[i] = u < 1 ? 1 : u;
+        sum += pmf[i];
+    }
+    /* force the sum to 128 one unit at a time on the first maximal entry (encoder.py:281-287) */
+    while (sum != 128) {
+        int best = 0;
+        for (int i = 1; i < nv; i++)
+            if (pmf[i] > pmf[best]) best = i;
+        if (sum > 128) { pmf[best]--; sum--; } else { pmf[best]++; sum++; }
+    }
+    /* cdf over min..max+1 with absent values given zero width (encoder.py:294-304) */
+    const int minv = vals[0] - 128, maxv = vals[nv - 1] - 128;
+    *min_value = minv;
+    *ncdf = maxv - minv + 2;
+    memset(cdf, 0, (size_t)*ncdf);
+    uint32_t left = 0;
+    int last = 0;
+    for (int i = 0; i < nv; i++) {
+        const int idx = vals[i] - 128 - minv;
+        for (int k = last + 1; k < idx + 1; k++) cdf[k] = (uint8_t)left;
+        last = idx;
+        left += pmf[i];
+    }
+    cdf[*ncdf - 1] = 128;
+    return ORC_OK;
+}
+
+typedef struct { uint32_t *w; int64_t n, cap; } orc_vec;
+
+static int vec_push(orc_vec *v, uint32_t x)
+{
+    if (v->n == v->cap) {
+        int64_t cap = v->cap ? 2 * v->cap : 1024;
+        uint32_t *p = (uint32_t *)realloc(v->w, (size_t)cap * 4);
+        if (!p) return ORC_ERR_OVERFLOW;
+        v->w = p;
+        v->cap = cap;
+    }
+    v->w[v->n++] = x;
+    return ORC_OK;
+}
+
+int orc_awr_encode(const int8_t *W, int64_t rows, int64_t cols, uint32_t **comp_out, int64_t *n_words,
+                   uint32_t *offsets, uint32_t *ppf, uint32_t *cum, uint32_t *prob)
+{
+    if (cols % 128 != 0 || rows <= 0) return ORC_ERR_SHAPE;
+    int minv = 0, ncdf = 0;
+    uint8_t cdf[260];
+    int rc = awr_fit(W, rows * cols, &minv, cdf, &ncdf);
+    if (rc) return rc;
+    orc_vec out = {0, 0, 0}, buf = {0, 0, 0};
+    uint32_t *un = NULL;
+    int64_t un_cap = 0;
+    uint64_t state[32];
+    memset(state, 0, sizeof state);  /* the 32 coders carry their states from row to row (encoder.py:402) */
+    for (int64_t r = 0; r < rows && !rc; r++) {
+        if (out.n / 4 > 0xFFFFFFFFll) { rc = ORC_ERR_OVERFLOW; break; }
+        offsets[r] = (uint32_t)(out.n / 4);
+        buf.n = 0;
+        const int8_t *row = W + r * cols;
+        for (int64_t c = cols / 128 - 1; c >= 0 && !rc; c--)
+            for (int l = 31; l >= 0 && !rc; l--) {
+                const int8_t *qd = row + 128 * c + 4 * l;
+                uint32_t lft[4], p[4];
+                uint64_t total = 1;
+                for (int i = 0; i < 4; i++) {
+                    const int idx = qd[i] - minv;
+                    lft[i] = cdf[idx];
+                    p[i] = (uint32_t)cdf[idx + 1] - lft[i];
+                    total *= p[i];
+                }
+                uint64_t s = state[l];
+                if ((s >> 36) >= total) {  /* flush one word (encoder.py:208-211) */
+                    rc = vec_push(&buf, (uint32_t)s);
+                    s >>= 32;
+                } else if (s == 0) {       /* first quad of the coder (encoder.py:212-217) */
+                    s = total << 4;
+                }
+                uint64_t concat = 0;
+                for (int i = 0; i < 4; i++) {
+                    const uint64_t rem = s % p[i];
+                    s /= p[i];
+                    concat |= (uint64_t)(lft[i] + rem) << (7 * i);
+                }
+                state[l] = (s << 28) | concat;
+            }
+        /* per row (encoder.py:431-447): reverse, pad to 64 (mod 128), state words at 64, transpose blocks */
+        const int64_t nb = buf.n;
+        const int64_t pad = ((64 - nb) % 128 + 128) % 128;
+        const int64_t tot = nb + pad + 64;
+        if (tot > un_cap) {
+            uint32_t *p = (uint32_t *)realloc(un, (size_t)tot * 4);
+            if (!p) { rc = ORC_ERR_OVERFLOW; break; }
+            un = p;
+            un_cap = tot;
+        }
+        int64_t k = 0;
+        for (int64_t i = 0; i < 64; i++) un[k++] = i < nb ? buf.w[nb - 1 - i] : 0u;
+        for (int l = 0; l < 32; l++) un[k++] = (uint32_t)state[l];
+        for (int l = 0; l < 32; l++) un[k++] = (uint32_t)(state[l] >> 32);
+        for (int64_t i = 64; i < nb + pad; i++) un[k++] = i < nb ? buf.w[nb - 1 - i] : 0u;
+        for (int64_t b = 0; b < tot / 128 && !rc; b++)
+            for (int l = 0; l < 32 && !rc; l++)
+                for (int f = 0; f < 4 && !rc; f++) rc = vec_push(&out, un[b * 128 + f * 32 + l]);
+    }
+    free(un);
+    free(buf.w);
+    if (rc) { free(out.w); return rc; }
+    /* decoder tables (encoder.py:309-320), packed 4 bytes per word little-endian (:464-470) */
+    uint8_t p8[128], c8[128], r8[128];
+    memset(p8, 0, sizeof p8); memset(c8, 0, sizeof c8); memset(r8, 0, sizeof r8);
+    for (int idx = 0; idx + 1 < ncdf; idx++)
+        for (uint32_t q = cdf[idx]; q < cdf[idx + 1]; q++) {
+            p8[q] = (uint8_t)(int8_t)(idx + minv);
+            c8[q] = cdf[idx];
+            r8[q] = (uint8_t)(cdf[idx + 1] - cdf[idx]);
+        }
+    for (int i = 0; i < 32; i++) {
+        ppf[i] = cum[i] = prob[i] = 0;
+        for (int b = 0; b < 4; b++) {
+            ppf[i] |= (uint32_t)p8[4 * i + b] << (8 * b);
+            cum[i] |= (uint32_t)c8[4 * i + b] << (8 * b);
+            prob[i] |= (uint32_t)r8[4 * i + b] << (8 * b);
+        }
+    }
+    *comp_out = out.w;
+    *n_words = out.n;
+    return ORC_OK;
+}
+
+void orc_free(void *p) { free(p); }

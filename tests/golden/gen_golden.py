@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference's own encoders.
 
-Run once, in a container that has the reference checkout (default
-/root/reference, override with MATVANS_REFERENCE):
+Run once, in a container that has the reference checkout, naming its root
+with --reference or the MATVANS_REFERENCE environment variable:
 
-    python tests/golden/gen_golden.py
+    python tests/golden/gen_golden.py --reference PATH/TO/MatVANS
 
 It imports the reference's Python encoders unchanged and records their outputs:
 
@@ -59,7 +59,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("MATVANS_REFERENCE", "/root/reference")
+REF = None  # the reference checkout's root (--reference or MATVANS_REFERENCE), set by main()
 
 
 def load_awr_encoder():
@@ -206,8 +206,19 @@ def gen_wpr(workdir):
 
 
 def main():
+    global REF
+    import argparse
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference", default=os.environ.get("MATVANS_REFERENCE"),
+                    help="root of the reference checkout (default: $MATVANS_REFERENCE)")
+    ap.add_argument("only", nargs="*", choices=["awr", "aws", "wpr"], help="fixture families (default: all)")
+    a = ap.parse_args()
+    if not a.reference or not os.path.isfile(os.path.join(a.reference, "buffered", "encoder.py")):
+        ap.error("the reference checkout is needed: pass --reference PATH (the directory holding buffered/ "
+                 "and matvansWarpPerRow/) or set MATVANS_REFERENCE")
+    REF = os.path.abspath(a.reference)
     enc = load_awr_encoder()
-    only = sys.argv[1:]
+    only = a.only
     if not only or "awr" in only:
         gen_awr(enc)
     if not only or "aws" in only:

@@ -151,3 +151,21 @@ def test_aws_rejects_bad_shape():
     c = _aws_cases()["s4_64x512"]
     with pytest.raises(oracle.OracleError):
         oracle.aws_decode(c["compressed"], c["offsets"], 48, 512, c["ppf"], c["ppf_cum"], c["ppf_prob"])
+
+
+def test_oracle_awr_encoder_matches_reference_encoder(awr_cases):
+    """The oracle's C restatement of the reference encoder (used by the benchmark's CPU legs, which must not
+    load the product library) is byte-identical to buffered/encoder.py on every reference-made fixture."""
+    for name, c in awr_cases.items():
+        comp, offs, ppf, cum, prob = oracle.awr_encode(c["W"])
+        assert np.array_equal(comp, c["compressed"]), name
+        assert np.array_equal(offs, c["offsets"]), name
+        for got, key in ((ppf, "ppf"), (cum, "ppf_cum"), (prob, "ppf_prob")):
+            assert np.array_equal(got, c[key]), (name, key)
+
+
+def test_oracle_awr_encoder_rejects_unencodable():
+    with pytest.raises(oracle.OracleError):
+        oracle.awr_encode(np.zeros((2, 100), np.int8))  # cols % 128 != 0 (encoder.py:397)
+    with pytest.raises(oracle.OracleError):
+        oracle.awr_encode(np.arange(-128, 128, dtype=np.int8).reshape(2, 128))  # > 128 distinct values
