@@ -36,9 +36,19 @@ SIGMAS = [4.0, 2.0]
 METRIC = "us/matvec & int8-equiv GB/s vs dense dp4a int8 on B200, bit-exact int32 output"
 UNIT = "GB/s"
 L2_BYTES = 126 * 2 ** 20
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the step's kernel (q8s_kernel, 8 warps, ilp 1),
-# from an ncu --set full capture of `bench.py --profile --tuning 8,1,1,0,0,0`
-STEP_DRAM_BYTES = 218.3e6
+# DRAM traffic of one launch of the step's kernel, as the latest committed ncu summary of it records
+PROFILE_RECORD = os.path.join(ROOT, "profiles", "q8s_kernel_stack12_b1.json")
+
+
+def profiled_traffic():
+    """(dram__bytes_read.sum + dram__bytes_write.sum per launch, source) from the committed profile record, or
+    (None, reason) when there is none."""
+    try:
+        with open(PROFILE_RECORD) as f:
+            rec = json.load(f)
+        return float(rec["dram_bytes_per_launch"]), f"{os.path.relpath(PROFILE_RECORD, ROOT)}: {rec['command']}"
+    except (OSError, ValueError, KeyError):
+        return None, "no profile record"
 
 
 def gen_matrix(shape, sigma, seed):
@@ -463,6 +473,128 @@ def large_section(torch, ops, autotune, dev, batches=(1, 16)):
     return out
 
 
+# ------------------------------------------------------------------ the reference's own CUDA kernels
+
+def _ref_libs():
+    """ctypes handles of the reference kernels built by oracle/build_ref.py (bench comparators), or {}."""
+    import ctypes
+    d = os.path.join(ROOT, "oracle", "_ref")
+    out = {}
+    for key, fn in (("awr", "libref_awr.so"), ("dense", "libref_dense.so"), ("wpr", "libref_wpr.so"),
+                    ("wpr_local", "libref_wpr_local.so")):
+        path = os.path.join(d, fn)
+        if os.path.exists(path):
+            out[key] = ctypes.CDLL(path)
+    return out
+
+
+def reference_kernels_section(torch, ops, dev, mats, xd, ours_us):
+    """The reference's own kernels (compiled unmodified for sm_100a by oracle/build_ref.py) on the sigma-4
+    matrices of the workload, each launched with the reference's own launch shape over rotating copies (cold
+    L2), next to this library's kernels on the same matrices.  Every stream buffer is padded so that the
+    kernels' known over-reads past a row's end stay inside it.  Gates: dense and WPR int32 y exact; AWR's
+    int8 output equal to clamp(rn(fp32(y) * scale))."""
+    import ctypes
+    libs = _ref_libs()
+    if not libs:
+        return {"unavailable": "oracle/_ref was not built (the reference checkout was absent at build time)"}
+    P = ctypes.c_void_p
+    stream = lambda: P(torch.cuda.current_stream().cuda_stream)  # noqa: E731
+    out = {}
+    for m in mats:
+        if m["sigma"] != 4.0:
+            continue
+        rows, cols = m["shape"]
+        key = f"{rows}x{cols}"
+        row = {}
+        W = m["W"]
+        x1 = xd[cols]
+        y_exact = (W.astype(np.int32) @ x1.cpu().numpy().astype(np.int32)).astype(np.int32)
+        if "dense" in libs:
+            L = libs["dense"]
+            Wd = torch.from_numpy(W).to(dev)
+            Ws = [Wd] + [Wd.clone() for _ in range(copies_for(rows * cols) - 1)]
+            yd = torch.empty(rows, dtype=torch.int32, device=dev)
+            run = lambda w: L.ref_dense_launch(P(yd.data_ptr()), P(w.data_ptr()), P(x1.data_ptr()), cols, rows,  # noqa
+                                               stream())
+            if run(Wd) != 0:
+                row["dense_dp4a"] = "launch failed"
+            else:
+                torch.cuda.synchronize()
+                if not np.array_equal(yd.cpu().numpy(), y_exact):
+                    row["dense_dp4a"] = "output differs from the exact product"
+                else:
+                    t = time_graph_med(torch, lambda: [run(w) for w in Ws], 10, inner=len(Ws))
+                    row["dense_dp4a_us"] = round(1e3 * t, 2)
+            del Ws, Wd
+        if "awr" in libs:
+            L = libs["awr"]
+            A = ops.AwrMatrix.encode(W, device=dev)
+            pad = 1024  # words past the stream: a row's last refill reads 32 uint4 ahead
+
+            def padded():
+                c = torch.zeros(A.n_words + pad, dtype=torch.int32, device=dev)
+                c[:A.n_words].copy_(A.compressed.view(torch.int32))
+                return c
+            comps = [padded() for _ in range(copies_for(4 * A.n_words))]
+            out8 = torch.empty(rows, dtype=torch.int8, device=dev)
+            scale = np.float32(127.0) / np.float32(max(1, int(np.abs(y_exact).max())))
+            run = lambda c: L.ref_awr_launch(P(out8.data_ptr()), P(c.data_ptr()), P(A.offsets.data_ptr()),  # noqa
+                                             P(A.ppf.data_ptr()), P(A.ppf_cum.data_ptr()), P(A.ppf_prob.data_ptr()),
+                                             P(x1.data_ptr()), cols, rows, ctypes.c_float(float(scale)), stream())
+            if run(comps[0]) != 0:
+                row["ans_warp_rows"] = "launch failed"
+            else:
+                torch.cuda.synchronize()
+                ref8 = np.clip(np.rint(y_exact.astype(np.float32) * scale), -128, 127).astype(np.int8)
+                if not np.array_equal(out8.cpu().numpy(), ref8):
+                    row["ans_warp_rows"] = "output differs from clamp(rn(y * scale))"
+                else:
+                    t = time_graph_med(torch, lambda: [run(c) for c in comps], 5, inner=len(comps))
+                    row["ans_warp_rows_us"] = round(1e3 * t, 2)
+            del comps, A
+        if rows == cols and cols % 512 == 0 and cols <= 4096 and ("wpr" in libs or "wpr_local" in libs):
+            Pm = ops.WprMatrix.encode(W, device=dev)
+
+            def padded_payload():
+                c = torch.zeros(Pm.payload_size + 4096, dtype=torch.int16, device=dev)
+                c[:Pm.payload_size].copy_(Pm.payload[:Pm.payload_size].view(torch.int16))
+                return c
+            pays = [padded_payload() for _ in range(copies_for(2 * Pm.payload_size))]
+            yw = torch.empty(rows, dtype=torch.int32, device=dev)
+            for name in ("wpr", "wpr_local"):
+                if name not in libs:
+                    continue
+                L = libs[name]
+                run = lambda p, L=L: L.ref_wpr_launch(  # noqa: E731
+                    P(yw.data_ptr()), P(x1.data_ptr()), rows, cols, P(Pm.cursors.data_ptr()),
+                    ctypes.c_int8(Pm.min_value), ctypes.c_uint8(Pm.G), P(Pm.cdf.data_ptr()), P(Pm.ppf.data_ptr()),
+                    P(p.data_ptr()), Pm.payload_size, stream())
+                label = "matvansWarpPerRow" if name == "wpr" else "matvansWarpPerRow_local_cdf"
+                if run(pays[0]) != 0:
+                    row[label] = "launch failed"
+                    continue
+                torch.cuda.synchronize()
+                if not np.array_equal(yw.cpu().numpy(), y_exact):
+                    row[label] = "output differs from the exact product"
+                    continue
+                t = time_graph_med(torch, lambda: [run(p) for p in pays], 5, inner=len(pays))
+                row[label + "_us"] = round(1e3 * t, 2)
+            del pays, Pm
+        for k, v in ours_us.items():
+            if k.startswith(key + "_s4_"):
+                row[f"ours_{k.split('_')[-1]}_us"] = round(v, 2)
+        best = min((v for k, v in ours_us.items() if k.startswith(key + "_s4_")), default=None)
+        if best:
+            for k in ("dense_dp4a_us", "ans_warp_rows_us", "matvansWarpPerRow_us", "matvansWarpPerRow_local_cdf_us"):
+                if k in row:
+                    row["speedup_vs_" + k[:-3]] = round(row[k] / best, 3)
+        out[key] = row
+        torch.cuda.empty_cache()
+    ops.device_status()
+    return out
+
+
 # ------------------------------------------------------------------ GPU arm
 
 def time_graph(torch, fn, reps, inner=1):
@@ -485,6 +617,22 @@ def time_graph(torch, fn, reps, inner=1):
     e1.record()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps / inner, g
+
+
+def time_graph_med(torch, fn, reps, inner=1, windows=10):
+    """Like time_graph, but the median over `windows` windows of `reps` replays (ms per fn() call / inner)."""
+    _, g = time_graph(torch, fn, 1, inner)
+    ts = []
+    for _ in range(windows):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / reps / inner)
+    del g
+    return float(np.median(ts))
 
 
 def copies_for(nbytes):
@@ -555,19 +703,26 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     sampler = ClockSampler(local)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # exactly K steps between a barrier + synchronize on both sides, recorded in >= 10 windows; the step
+    # time is the median window (per-window means), and the job's time the slowest rank's
+    nwin = max(1, min(10, args.steps))
+    bounds = [round(i * args.steps / nwin) for i in range(nwin + 1)]
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(nwin + 1)]
     mvd.barrier()
     torch.cuda.synchronize()
     with sampler:
-        e0.record()
-        for _ in range(args.steps):
-            g.replay()
-        e1.record()
+        evs[0].record()
+        for w in range(nwin):
+            for _ in range(bounds[w + 1] - bounds[w]):
+                g.replay()
+            evs[w + 1].record()
         torch.cuda.synchronize()
     mvd.barrier()
+    win_ms = [evs[w].elapsed_time(evs[w + 1]) / max(1, bounds[w + 1] - bounds[w]) for w in range(nwin)]
     step_bytes = sum(int8_equiv_bytes(e["rows"], e["cols"]) for e in entries)
-    value, sec = mvd.aggregate_throughput(step_bytes / 1e9, e0.elapsed_time(e1) / args.steps * 1e-3, device=dev)
+    value, sec = mvd.aggregate_throughput(step_bytes / 1e9, float(np.median(win_ms)) * 1e-3, device=dev)
     ms = sec * 1e3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     alg = sum(e["alg_bytes"] for e in entries)
     peak, peak_kind = measured_peak()
     achieved = alg / (ms * 1e-3) / 1e9
@@ -615,8 +770,12 @@ def run_ours(args):
     per = {}
     for e in (entries if extras else []):
         M = e["M"]
-        tun, info = autotune.tune(M, batch=1)
-        t_ms = info["us"] * 1e-3
+        tun, _ = autotune.tune(M, batch=1)  # the launch shape may come from the cache; the time is taken here
+        Ms = autotune.copies(M, copies_for(M.payload_bytes))
+        x1 = xd[e["cols"]][None]
+        y1 = torch.empty((1, e["rows"]), dtype=torch.int32, device=dev)
+        t_ms = time_graph_med(torch, lambda: [Mi.matvec(x1, out=y1, tuning=tun) for Mi in Ms], 10, inner=len(Ms))
+        del Ms
         per[e["name"]] = {"us": 1e3 * t_ms, "int8_equiv_gbs": int8_equiv_bytes(e["rows"], e["cols"]) / t_ms / 1e6,
                           "compressed_gbs": e["alg_bytes"] / t_ms / 1e6, "bits_per_weight": M.bits_per_weight,
                           "entropy_bits": e["entropy"],
@@ -671,6 +830,9 @@ def run_ours(args):
             del Ps, P
         torch.cuda.empty_cache()
 
+    ref_kernels = reference_kernels_section(torch, ops, dev, mats, xd, {k: v["us"] for k, v in per.items()}) \
+        if extras else None
+
     # float form (configs[3] shapes): forward and re-decoding backward, us per call
     float_form = {}
     for m in (mats if extras else []):
@@ -694,6 +856,7 @@ def run_ours(args):
     large = None if (args.no_stack or not extras) else large_section(torch, ops, autotune, dev)
 
 
+    traffic, traffic_src = profiled_traffic()
     line = None
     if rank == 0:
         cb = None
@@ -711,6 +874,8 @@ def run_ours(args):
             "stack_tuning": list(stack_tuning), "stack_candidates_us": stack_cands,
             "us_per_matvec": {k: round(v["us"], 3) for k, v in per.items()},
             "per_matrix": per,
+            "reference_kernels": ref_kernels,
+            "step_windows_ms": [round(v, 4) for v in win_ms],
             "dense_dp4a": dense, "cublas_sgemv_fp32": cublas, "ans_warp_rows_kernel": awr_t,
             "warp_per_row_kernel": wpr_t,
             "ans_warp_stripes_kernel": aws_t,
@@ -720,7 +885,8 @@ def run_ours(args):
             "speedup_vs_dense_dp4a": {k: round(dense[k.split("_s")[0]]["us"] / v["us"], 3)
                                       for k, v in per.items() if k.split("_s")[0] in dense and "_s4_" in k},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": STEP_DRAM_BYTES, "traffic_unit": "bytes per launch",
+                         "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes per launch",
+                         "traffic_source": traffic_src,
                          "algorithmic_bytes": alg, "peak_kind": peak_kind,
                          "kernel": "q8s_kernel<1,ILP,DEPTH> (mv_q8_stack_matvec)",
                          "note": "algorithmic bytes = compressed streams + tables + offsets + x + int32 y"},

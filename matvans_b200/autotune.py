@@ -90,7 +90,8 @@ def key(M, batch):
             f"|bpw{M.bits_per_weight:.1f}|B{batch}")
 
 
-def _copies(M, n):
+def copies(M, n):
+    """M and n - 1 device copies of its encoding (cold-L2 timing)."""
     from .ops import Q8Matrix
     enc = {"rows": M.rows, "cols": M.cols, "blocks": M.blocks.cpu().numpy(), "blk_off": M.blk_off.cpu().numpy(),
            "tbl": M.tbl.cpu().numpy().view(np.uint16), "tbl_off": M.tbl_off.cpu().numpy(),
@@ -133,7 +134,7 @@ def tune(M, batch=1, candidates=None, reps=10, force=False):
     if not force and k in db:
         return Q8Tuning(*db[k]["tuning"]), db[k]
     R = int(min(48, max(2, -(-2 * L2_BYTES // max(1, M.payload_bytes)))))
-    mats = _copies(M, R)
+    mats = copies(M, R)
     x = torch.randint(-127, 128, (batch, M.cols), dtype=torch.int8, device=M.device)
     y = torch.empty((batch, M.rows), dtype=torch.int32, device=M.device)
     results = {}
