@@ -389,6 +389,12 @@ mv_status mv_read_wpr_bin(const char *path, mv_blob **out);
 #define MV_INJECT_DROP_COPY 2
 mv_status mv_debug_inject(int what, uint32_t value);
 
+/* Test and debugging aid (no reference counterpart): MV_QUERY_STATUS_WORD sets
+ * *value to 1 if the current device's status word (the library's only lazily
+ * created device allocation) exists, else 0; it creates nothing. */
+#define MV_QUERY_STATUS_WORD 1
+mv_status mv_debug_query(int what, uint64_t *value);
+
 /* FxHash-style hash of an int8 vector (buffered/encoder.py:8-20). */
 uint32_t mv_hash_int8(const int8_t *v, size_t n);
 

@@ -26,7 +26,7 @@ EXPORTS = [
     "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc", "mv_q8_matvec_tuned", "mv_q8_stack_plan",
     "mv_q8_stack_matvec", "mv_q8_matvec_bf16", "mv_q8_matvec_t_bf16", "mv_q8_chain_plan", "mv_q8_chain_matvec",
     "mv_aws_matvec", "mv_aws_matvec_requant", "mv_aws_encode", "mat_vec_mul_coalesced_stripes",
-    "mv_q8_x_tiles_bytes",
+    "mv_q8_x_tiles_bytes", "mv_debug_query",
 ]
 
 
@@ -114,6 +114,7 @@ def lib():
         "mv_read_wpr_bin": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)], st),
         "mv_hash_int8": ([P, sz], ctypes.c_uint32),
         "mv_debug_inject": ([i32, ctypes.c_uint32], st),
+        "mv_debug_query": ([i32, ctypes.POINTER(ctypes.c_uint64)], st),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

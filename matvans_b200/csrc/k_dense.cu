@@ -235,6 +235,17 @@ mv_status mv_debug_inject(int what, uint32_t value) {
     return MV_OK;
 }
 
+mv_status mv_debug_query(int what, uint64_t *value) {
+    if (!value) return mv::fail(MV_ERR_ARG, "mv_debug_query: NULL value");
+    if (what != MV_QUERY_STATUS_WORD) return mv::fail(MV_ERR_ARG, "mv_debug_query: unknown key %d", what);
+    int d = 0;
+    MV_CUDA_TRY(cudaGetDevice(&d), "cudaGetDevice");
+    if (d < 0 || d >= 64) return mv::fail(MV_ERR_ARG, "mv_debug_query: device %d out of range", d);
+    std::lock_guard<std::mutex> lk(mv::g_mu);
+    *value = mv::g_dev[d].status ? 1u : 0u;
+    return MV_OK;
+}
+
 mv_status mv_device_status(void *stream, uint32_t *flags) {
     if (!flags) return mv::fail(MV_ERR_ARG, "mv_device_status: NULL flags");
     mv_status rc;

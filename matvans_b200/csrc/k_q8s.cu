@@ -4,17 +4,23 @@
 // Work item = (job, stripe, segment group).  A group is SG = W*ILP segments
 // of one stripe: warp w decodes segments g*SG + w (+ W) -- with ILP = 2 the
 // two segments are independent rANS streams interleaved in one instruction
-// stream, which hides the ~100-cycle latency chain of a decode step.  CTAs are
-// persistent and take items c, c + G, c + 2G, ... .
+// stream, which hides the ~60-cycle latency chain of a decode step.  CTAs are
+// persistent.  A stack takes its items from a work queue (one global counter,
+// numbered job by job, so that consecutive items of a CTA usually share a
+// global table); single matrices and chains take items c, c + G, c + 2G, ... .
+// Thread 0 keeps the CTA's next two items in a small shared-memory ring, so
+// that warps can copy their streams one item ahead.
 //
 // Per item:
 //   * lane 0 of each warp moves the warp's stream blocks into shared memory
 //     with 1-D bulk copies (cp.async.bulk, TMA engine, no multicast) completing
-//     on an mbarrier; with DEPTH = 2 the copies of the CTA's next item are in
-//     flight while the current one is decoded;
+//     on an mbarrier, DEPTH steps ahead of its decode (across item boundaries);
 //   * the decode table (256 quantiles x 32 lanes, conflict-free) is rebuilt
 //     only when the table changes: every item for per-row tables, once per
-//     job for a global table.  CUDA-core consumers use the wide layout, 8-byte
+//     job for a global table.  The table data of the next item is staged in
+//     shared memory by asynchronous copies (cp.async) while the current item
+//     decodes, so a rebuild does not wait for device memory.  CUDA-core
+//     consumers use the wide layout, 8-byte
 //     entries {f | sym << 16, r} at byte q*256 + l*8 (64 KB): one byte permute
 //     of the state gives a lookup address and r needs no extraction.  The
 //     tensor-core consumers, two CTAs per SM, keep the narrow layout, 4-byte
@@ -26,7 +32,9 @@
 //
 // Decode step (per lane, per quad of 4 symbols; table entry e = f | sym << 16
 // | r << 24 with f the symbol's frequency, r = q - cum < f <= 255):
-//   refill:   if (hi == 0) { hi = lo; lo = next word }
+//   refill:   if (hi == 0) { hi = lo; lo = next word } -- the lane's stream
+//             position is a shared-memory byte offset that advances by one
+//             128-byte word-row, clamped to the row after the block
 //   lookups:  e_i = table[byte i of lo]
 //   update:   u01 = r0 + f0*r1, t2 = r2 + f2*r3, f0*f1, f2*f3 (dp2a: 16-bit
 //             x 8-bit dot products read f straight from the entries), t0 =
@@ -43,6 +51,13 @@
 namespace mv {
 
 typedef mv_q8_job Q8Job;
+
+// Shared-memory layout of q8s_kernel (byte offsets; see q8s_layout).
+constexpr uint32_t kStageOffs = 40;  // u32 per staging area: 33 relative offsets, [36] valid, [37] first entry
+constexpr uint32_t kStagePad = 8;    // entries per staging area beyond tbl_stage (copies start at an even entry)
+struct Q8SLayout {
+    uint32_t extra, bufs, red, bars, ring, curs, sched, stage_o, rows, stage_e, total;
+};
 
 __global__ void scale_rows_kernel(const int32_t *y, const float *s, float *ys, int rows, int batch, int ldy);
 
@@ -63,30 +78,21 @@ struct Q8SLaunch {
     // j+1's x (the last job's goes to chain_out8); jobs[j].pad counts job j's finished work items
     const float *chain_scales;
     int8_t *chain_out8;
+    // work queue of a stack (jobs[0].pad of the job table), or nullptr: static round robin
+    uint32_t *queue;
+    // shared-memory layout of this launch (set by the launcher; constant-bank operands in the kernel)
+    Q8SLayout lay;
+    uint32_t slot_bytes;  // ILP * buf_words * 4: one warp's stream slot
+    uint32_t stage_len;   // entries per table staging area
 };
 
-struct ItemInfo {
-    int job, stripe, group;
+// One work item as the CTA's scheduler hands it out (it < 0: no more items).
+struct alignas(16) ItemRec {
+    int32_t it, job, stripe, sb, se, pad0, pad1, pad2;
 };
+constexpr int kRing = 4;  // items the ring holds: the current one and up to two ahead
 
 __device__ __forceinline__ const Q8Job &job_at(const Q8SLaunch &L, int j) { return L.jobs ? L.jobs[j] : L.job0; }
-
-__device__ __forceinline__ ItemInfo find_item(const Q8SLaunch &L, uint32_t it) {
-    if (!L.jobs) {
-        const int ng = L.job0.ngroups;
-        return ItemInfo{0, (int)(it / ng), (int)(it % ng)};
-    }
-    const Q8Job *jobs = L.jobs;
-    int lo = 0, hi = L.njobs - 1;
-    while (lo < hi) {  // last job with item0 <= it
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&jobs[mid].item0) <= it) lo = mid;
-        else hi = mid - 1;
-    }
-    const uint32_t rel = it - __ldg(&jobs[lo].item0);
-    const int ng = __ldg(&jobs[lo].ngroups);
-    return ItemInfo{lo, (int)(rel / ng), (int)(rel % ng)};
-}
 
 // Segment range [sb, se) of an item: its stripe's segments split into ngroups parts.
 __device__ __forceinline__ void item_segs(const mv_q8_view &m, int ngroups, int group, int &sb, int &se) {
@@ -95,38 +101,99 @@ __device__ __forceinline__ void item_segs(const mv_q8_view &m, int ngroups, int 
     se = min(m.nseg, sb + spp);
 }
 
+// Item number -> record.  Each CTA takes its items in increasing order, so the job search runs forward from
+// the previous item's job (jhint): one comparison in the common case, a binary search over the rest otherwise.
+__device__ __forceinline__ ItemRec make_item(const Q8SLaunch &L, uint32_t it, int &jhint) {
+    ItemRec r{};
+    if (it >= L.nitems) {
+        r.it = -1;
+        return r;
+    }
+    int j = 0;
+    uint32_t rel = it;
+    int ng = L.job0.ngroups;
+    if (L.jobs) {
+        j = jhint;
+        if (j + 1 < L.njobs && __ldg(&L.jobs[j + 1].item0) <= it) {
+            int lo = j + 1, hi = L.njobs - 1;
+            while (lo < hi) {  // last job with item0 <= it
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&L.jobs[mid].item0) <= it) lo = mid;
+                else hi = mid - 1;
+            }
+            j = lo;
+        }
+        jhint = j;
+        rel = it - __ldg(&L.jobs[j].item0);
+        ng = __ldg(&L.jobs[j].ngroups);
+    }
+    r.it = (int32_t)it;
+    r.job = j;
+    r.stripe = (int)(rel / (uint32_t)ng);
+    item_segs(job_at(L, j).m, ng, (int)(rel % (uint32_t)ng), r.sb, r.se);
+    return r;
+}
+
+// The CTA's k-th item number (thread 0 only).  Static: c + k G.  Queue: one atomic per item; every CTA takes
+// items until one grab fails, so a launch makes exactly nitems + G grabs, and the one that makes the last of
+// them (no other grab can follow it) resets the counter for the next launch.
+__device__ __forceinline__ uint32_t sched_grab(const Q8SLaunch &L, uint32_t k) {
+    if (!L.queue) {
+        const unsigned long long v = (unsigned long long)blockIdx.x + (unsigned long long)k * gridDim.x;
+        return v < L.nitems ? (uint32_t)v : L.nitems;
+    }
+    return atomicAdd(L.queue, 1u);
+}
+__device__ __forceinline__ void sched_after_grab(const Q8SLaunch &L, uint32_t v) {
+    if (L.queue && v == L.nitems + gridDim.x - 1) atomicExch(L.queue, 0u);
+}
+
 // Steps of a warp in an item of n segments; step j covers segments
 // sb + warp + j*W*ILP + k*W for k < ILP.
 __device__ __forceinline__ int warp_steps(int n, int warp, int W, int ILP) {
     return warp < n ? (n - warp + W * ILP - 1) / (W * ILP) : 0;
 }
 
-// The next (item, step) of one warp's stream of segments, tracked by lane 0.
-struct StepCursor {
-    uint32_t it;
-    int j, steps, sb, se, stripe, job;
+// The next step whose stream blocks a warp copies (lane 0; kept in shared memory): ring index k of its
+// item, step j of `steps`.  An item's record may be read once it is visible (written before a CTA barrier the
+// warp has passed).
+struct alignas(16) StepCursor {
+    int k, j, steps, sb, se, stripe, job, done;
 };
 
-__device__ __forceinline__ void cursor_seek(StepCursor &c, const Q8SLaunch &L, uint32_t it, int warp, int W,
-                                            int ILP) {
-    for (; it < L.nitems; it += gridDim.x) {
-        const ItemInfo I = find_item(L, it);
-        const Q8Job &J = job_at(L, I.job);
-        int sb, se;
-        item_segs(J.m, J.ngroups, I.group, sb, se);
-        const int steps = warp_steps(se - sb, warp, W, ILP);
-        if (steps > 0) {
-            c = StepCursor{it, 0, steps, sb, se, I.stripe, I.job};
-            return;
+// Thread 0's scheduler state, kept in shared memory (off the decode loop's registers).
+struct alignas(16) SchedState {
+    uint32_t ngrab, pending;
+    int jhint, grab_done, grab_now, pad0, pad1, pad2;
+};
+
+// Moves the cursor onto a step that exists (entering later items while they are visible); false while the
+// next item is not visible yet.
+__device__ __forceinline__ bool cursor_ready(StepCursor &c, const ItemRec *ring, int kvis, int warp, int W,
+                                             int ILP) {
+    while (!c.done && c.j >= c.steps) {
+        if (c.k + 1 > kvis) return false;
+        c.k++;
+        const ItemRec &I = ring[c.k % kRing];
+        if (I.it < 0) {
+            c.done = 1;
+            break;
         }
+        c.j = 0;
+        c.steps = warp_steps(I.se - I.sb, warp, W, ILP);
+        c.sb = I.sb;
+        c.se = I.se;
+        c.stripe = I.stripe;
+        c.job = I.job;
     }
-    c.it = L.nitems;
+    return !c.done;
 }
 
-// Issue the bulk copies of the cursor's step into one slot (lane 0 only).
+// Issue the bulk copies of the cursor's step into one slot (lane 0 only).  soff is the slot's byte offset in
+// shared memory.
 template <int ILP>
 __device__ __forceinline__ void issue_step(const Q8SLaunch &L, const StepCursor &c, int warp, int W,
-                                           uint32_t *slot_bufs, uint64_t *bar, uint32_t *rows_out) {
+                                           unsigned char *sm, uint32_t soff, uint64_t *bar, uint32_t *rows_out) {
     const mv_q8_view &m = job_at(L, c.job).m;
     const int seg0 = c.sb + warp + c.j * W * ILP;
     uint32_t total = 0;
@@ -154,7 +221,9 @@ __device__ __forceinline__ void issue_step(const Q8SLaunch &L, const StepCursor 
     if (!L.drop_copy) {
 #pragma unroll
         for (int k = 0; k < ILP; k++)
-            if (rows[k]) bulk_g2s(slot_bufs + k * L.buf_words, m.blocks + (size_t)o0s[k] * 32, rows[k] * 128u, bar);
+            if (rows[k])
+                bulk_g2s(sm + soff + (uint32_t)k * (uint32_t)L.buf_words * 4u, m.blocks + (size_t)o0s[k] * 32,
+                         rows[k] * 128u, bar);
     }
 }
 
@@ -194,15 +263,25 @@ __device__ __forceinline__ void dot4(uint32_t w, const uint4 (&xv)[NV], int j, i
     }
 }
 
+// Refill of one stream.  koff is the byte offset (from the start of shared memory) of the lane's next word:
+// it is read every step, and taken when the high half of the state is empty; the offset then moves one
+// 128-byte word-row on, never past kend (the row after the block), so a corrupt stream rereads that row and
+// fails the final-state check instead of leaving its slot.
+__device__ __forceinline__ void q8_refill(uint32_t &lo, uint32_t &hi, uint32_t &koff, const uint32_t kend,
+                                          const unsigned char *sm) {
+    const uint32_t w = *reinterpret_cast<const uint32_t *>(sm + koff);
+    if (hi == 0) {
+        hi = lo;
+        lo = w;
+        koff = __viaddmin_u32(koff, 128u, kend);
+    }
+}
+
 // One decode step of one stream; returns the packed four symbols.
-__device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t &kidx, const uint32_t kend,
-                                            const uint32_t *buf, const uint32_t *lut_l, uint32_t stride,
+__device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t &koff, const uint32_t kend,
+                                            const unsigned char *sm, const uint32_t *lut_l, uint32_t stride,
                                             uint32_t &P) {
-    const uint32_t w = buf[kidx];
-    const bool need = hi == 0;
-    hi = need ? lo : hi;
-    lo = need ? w : lo;
-    kidx = need ? min(kidx + 32, kend) : kidx;
+    q8_refill(lo, hi, koff, kend, sm);
     const uint32_t a0 = __byte_perm(lo, 0, 0x4440), a1 = __byte_perm(lo, 0, 0x4441);
     const uint32_t a2 = __byte_perm(lo, 0, 0x4442), a3 = __byte_perm(lo, 0, 0x4443);
     // stride is 32 words, passed at run time so the index math stays an IMAD
@@ -226,14 +305,9 @@ __device__ __forceinline__ uint32_t q8_step(uint32_t &lo, uint32_t &hi, uint32_t
 // The same step over the wide table: 8-byte entries {f | sym << 16, r} at byte q*256 + lane*8 from the
 // start of shared memory.  A quantile byte of the state lands in bits 8..15 of the address and lane*8 in
 // bits 0..7, so one byte permute forms each lookup address, and r arrives as a clean word.
-__device__ __forceinline__ uint32_t q8_step_wide(uint32_t &lo, uint32_t &hi, uint32_t &kidx, const uint32_t kend,
-                                                 const uint32_t *buf, const unsigned char *lut_b, uint32_t lane8,
-                                                 uint32_t &P) {
-    const uint32_t w = buf[kidx];
-    const bool need = hi == 0;
-    hi = need ? lo : hi;
-    lo = need ? w : lo;
-    kidx = need ? min(kidx + 32, kend) : kidx;
+__device__ __forceinline__ uint32_t q8_step_wide(uint32_t &lo, uint32_t &hi, uint32_t &koff, const uint32_t kend,
+                                                 const unsigned char *lut_b, uint32_t lane8, uint32_t &P) {
+    q8_refill(lo, hi, koff, kend, lut_b);  // the table and the stream slots share the shared-memory base
     const uint2 e0 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5504));
     const uint2 e1 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5514));
     const uint2 e2 = *reinterpret_cast<const uint2 *>(lut_b + __byte_perm(lo, lane8, 0x5524));
@@ -250,18 +324,33 @@ __device__ __forceinline__ uint32_t q8_step_wide(uint32_t &lo, uint32_t &hi, uin
     return __byte_perm(__byte_perm(e0.x, e1.x, 0x0062), __byte_perm(e2.x, e3.x, 0x0062), 0x5410);
 }
 
-// One step through whichever table layout the consumer uses; lut is the table base (wide) or the
-// lane's column (narrow).
+// One step through whichever table layout the consumer uses; sm is the start of shared memory (where the
+// wide table sits), lut the lane's column of the narrow table.
 template <bool kWide>
-__device__ __forceinline__ uint32_t q8_step_t(uint32_t &lo, uint32_t &hi, uint32_t &kidx, const uint32_t kend,
-                                              const uint32_t *buf, const uint32_t *lut, uint32_t stride, int lane,
+__device__ __forceinline__ uint32_t q8_step_t(uint32_t &lo, uint32_t &hi, uint32_t &koff, const uint32_t kend,
+                                              const unsigned char *sm, const uint32_t *lut, uint32_t stride, int lane,
                                               uint32_t &P) {
     if constexpr (kWide)
-        return q8_step_wide(lo, hi, kidx, kend, buf, reinterpret_cast<const unsigned char *>(lut),
-                            (uint32_t)lane << 3, P);
+        return q8_step_wide(lo, hi, koff, kend, sm, (uint32_t)lane << 3, P);
     else
-        return q8_step(lo, hi, kidx, kend, buf, lut, stride, P);
+        return q8_step(lo, hi, koff, kend, sm, lut, stride, P);
 }
+
+// Start of a segment's stream in the slot at byte offset soff: the lane's state (word-rows 0 and 1), the
+// offset of its first refill word (word-row 2) and the bound (the row after the block's `rows` rows).
+struct SegStream {
+    uint32_t lo, hi, koff, kend, P;
+    __device__ __forceinline__ SegStream(const unsigned char *sm, uint32_t soff, uint32_t rows, int lane) {
+        const uint32_t l4 = (uint32_t)lane * 4u;
+        lo = *reinterpret_cast<const uint32_t *>(sm + soff + l4);
+        hi = *reinterpret_cast<const uint32_t *>(sm + soff + 128u + l4);
+        koff = soff + 256u + l4;
+        kend = soff + rows * 128u + l4;
+        P = 0;
+    }
+    // the encoder starts every segment from the last quad's frequency product, so the decoder ends there
+    __device__ __forceinline__ bool ok() const { return hi == 0 && lo == P; }
+};
 
 // --------------------------------------------------------------- consumers
 // A consumer turns decoded quads (four int8 weights of the lane's row) into
@@ -274,6 +363,8 @@ template <int NV>
 struct IntCons {
     static constexpr int kNV = NV;
     static constexpr int kRedNV = NV;
+    static constexpr int kRedBufs = 2;          // alternating reduction areas: one CTA barrier per item
+    static constexpr bool kFinishSyncs = true;  // finish_item holds a CTA barrier
     static constexpr int kMinCtas = 1;
     static constexpr int kMaxThreads = 512;  // up to 16 warps per CTA
     static constexpr int kTmemCols = 0;
@@ -284,8 +375,8 @@ struct IntCons {
     __device__ __forceinline__ void drain(const Q8SLaunch &) {}
     template <int ILP>
     __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
-                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                             int lane);
+                                             const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                             uint32_t soff, const uint32_t *lut_l, int lane);
     const int8_t *x;
     int cols, job_idx;
     int acc[NV];
@@ -307,6 +398,9 @@ struct IntCons {
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = __dp4a((int)wq, (int)xv[v], acc[v]);
     }
+    // The CTA barrier here is the only one of an item without a table rebuild: `red` alternates between two
+    // areas, so the next item's partial sums never meet this item's readers.  Every warp has finished its
+    // decode at the barrier, so the decode table may be rebuilt right after it.
     __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
                                                 int W, void *red_smem) {
         int *red = reinterpret_cast<int *>(red_smem);
@@ -330,7 +424,8 @@ struct IntCons {
                 }
             }
         }
-        __syncthreads();  // red is reused by the next item
+        // a chain counts the item as done (thread 0, next) only after every output of it is stored
+        if (L.chain_scales) __syncthreads();
     }
 };
 
@@ -352,6 +447,8 @@ template <int NV>
 struct FwdCons {
     static constexpr int kNV = NV;
     static constexpr int kRedNV = NV;
+    static constexpr int kRedBufs = 1;
+    static constexpr bool kFinishSyncs = true;
     static constexpr int kMinCtas = 1;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
@@ -362,8 +459,8 @@ struct FwdCons {
     __device__ __forceinline__ void drain(const Q8SLaunch &) {}
     template <int ILP>
     __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
-                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                             int lane);
+                                             const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                             uint32_t soff, const uint32_t *lut_l, int lane);
     const uint16_t *x;
     int cols;
     float acc[NV];
@@ -439,6 +536,8 @@ template <int NV>
 struct BwdCons {
     static constexpr int kNV = NV;
     static constexpr int kRedNV = NV;
+    static constexpr int kRedBufs = 1;
+    static constexpr bool kFinishSyncs = false;  // no barrier in finish_item: the kernel adds one per item
     static constexpr int kMinCtas = 1;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
@@ -449,8 +548,8 @@ struct BwdCons {
     __device__ __forceinline__ void drain(const Q8SLaunch &) {}
     template <int ILP>
     __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
-                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                             int lane);
+                                             const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                             uint32_t soff, const uint32_t *lut_l, int lane);
     float g[NV];
     float *dx;
     int cols;
@@ -511,20 +610,18 @@ struct BwdCons {
 // Decode the ILP segments of one step, feeding every quad to the consumer.
 template <class Cons, int ILP>
 __device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
-                                            const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                            int lane, Cons &cons) {
+                                            const uint32_t (&rows_now)[ILP], const unsigned char *sm, uint32_t soff,
+                                            const uint32_t *lut_l, int lane, Cons &cons) {
+    constexpr bool kW = Cons::kWideLut;
     const int qtot = (m.cols + 3) >> 2;
     const int q0A = seg0 * m.seg_quads;
     const int nqA = rows_now[0] ? min(m.seg_quads, qtot - q0A) : 0;
-    uint32_t loA = sb[lane], hiA = sb[32 + lane], kA = 64 + lane, PA = 0;
-    const uint32_t kendA = rows_now[0] * 32 + lane;
+    SegStream A(sm, soff, rows_now[0], lane);
     int iA = 0;
     if (ILP == 2) {
-        uint32_t *sbB = sb + L.buf_words;
         const int q0B = (seg0 + W) * m.seg_quads;
         const int nqB = rows_now[ILP - 1] ? min(m.seg_quads, qtot - q0B) : 0;
-        uint32_t loB = sbB[lane], hiB = sbB[32 + lane], kB = 64 + lane, PB = 0;
-        const uint32_t kendB = rows_now[ILP - 1] * 32 + lane;
+        SegStream B(sm, soff + (uint32_t)L.buf_words * 4u, rows_now[ILP - 1], lane);
         const int nboth = min(nqA, nqB) & ~3;
         for (; iA < nboth; iA += 4) {
             typename Cons::Group ga, gb;
@@ -532,54 +629,54 @@ __device__ __forceinline__ void decode_step(const Q8SLaunch &L, const mv_q8_view
             cons.load_group(gb, q0B + iA);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                const uint32_t wa = q8_step_t<Cons::kWideLut>(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, lane, PA);
-                const uint32_t wb = q8_step_t<Cons::kWideLut>(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, lane, PB);
+                const uint32_t wa = q8_step_t<kW>(A.lo, A.hi, A.koff, A.kend, sm, lut_l, L.lut_stride, lane, A.P);
+                const uint32_t wb = q8_step_t<kW>(B.lo, B.hi, B.koff, B.kend, sm, lut_l, L.lut_stride, lane, B.P);
                 cons.use(ga, j, q0A + iA + j, wa, lane);
                 cons.use(gb, j, q0B + iA + j, wb, lane);
             }
         }
         for (int j = iA; j < nqB; j++) {
-            const uint32_t wb = q8_step_t<Cons::kWideLut>(loB, hiB, kB, kendB, sbB, lut_l, L.lut_stride, lane, PB);
+            const uint32_t wb = q8_step_t<kW>(B.lo, B.hi, B.koff, B.kend, sm, lut_l, L.lut_stride, lane, B.P);
             cons.single(q0B + j, wb, lane);
         }
-        if (nqB > 0 && (hiB != 0 || loB != PB)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+        if (nqB > 0 && !B.ok()) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
     for (; iA + 4 <= nqA; iA += 4) {
         typename Cons::Group ga;
         cons.load_group(ga, q0A + iA);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const uint32_t wa = q8_step_t<Cons::kWideLut>(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, lane, PA);
+            const uint32_t wa = q8_step_t<kW>(A.lo, A.hi, A.koff, A.kend, sm, lut_l, L.lut_stride, lane, A.P);
             cons.use(ga, j, q0A + iA + j, wa, lane);
         }
     }
     for (; iA < nqA; iA++) {
-        const uint32_t wa = q8_step_t<Cons::kWideLut>(loA, hiA, kA, kendA, sb, lut_l, L.lut_stride, lane, PA);
+        const uint32_t wa = q8_step_t<kW>(A.lo, A.hi, A.koff, A.kend, sm, lut_l, L.lut_stride, lane, A.P);
         cons.single(q0A + iA, wa, lane);
     }
-    if (nqA > 0 && (hiA != 0 || loA != PA)) atomicOr(L.status, MV_DEV_FINAL_STATE);
+    if (nqA > 0 && !A.ok()) atomicOr(L.status, MV_DEV_FINAL_STATE);
 }
 
 template <int NV>
 template <int ILP>
 __device__ __forceinline__ void IntCons<NV>::run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
-                                                      const uint32_t (&rows_now)[ILP], uint32_t *sb,
-                                                      const uint32_t *lut_l, int lane) {
-    decode_step<IntCons<NV>, ILP>(L, m, seg0, W, rows_now, sb, lut_l, lane, *this);
+                                                      const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                                      uint32_t soff, const uint32_t *lut_l, int lane) {
+    decode_step<IntCons<NV>, ILP>(L, m, seg0, W, rows_now, sm, soff, lut_l, lane, *this);
 }
 template <int NV>
 template <int ILP>
 __device__ __forceinline__ void FwdCons<NV>::run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
-                                                      const uint32_t (&rows_now)[ILP], uint32_t *sb,
-                                                      const uint32_t *lut_l, int lane) {
-    decode_step<FwdCons<NV>, ILP>(L, m, seg0, W, rows_now, sb, lut_l, lane, *this);
+                                                      const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                                      uint32_t soff, const uint32_t *lut_l, int lane) {
+    decode_step<FwdCons<NV>, ILP>(L, m, seg0, W, rows_now, sm, soff, lut_l, lane, *this);
 }
 template <int NV>
 template <int ILP>
 __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int W,
-                                                      const uint32_t (&rows_now)[ILP], uint32_t *sb,
-                                                      const uint32_t *lut_l, int lane) {
-    decode_step<BwdCons<NV>, ILP>(L, m, seg0, W, rows_now, sb, lut_l, lane, *this);
+                                                      const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                                      uint32_t soff, const uint32_t *lut_l, int lane) {
+    decode_step<BwdCons<NV>, ILP>(L, m, seg0, W, rows_now, sm, soff, lut_l, lane, *this);
 }
 
 // y = W x for 8..16 int8 vectors on the tensor cores.  Every 16 decoded quads
@@ -602,6 +699,8 @@ __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const 
 struct MmaCons {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;      // reduction area: the x tiles
+    static constexpr int kRedBufs = 1;
+    static constexpr bool kFinishSyncs = true;
     static constexpr int kMinCtas = 1;    // with up to 16 warps: at most 128 registers per thread
     static constexpr int kMaxThreads = 512;  // 1 x 16 or 2 x 8 warps per SM
     static constexpr int kTmemCols = 1;   // > 0: the kernel allocates TMEM
@@ -725,8 +824,8 @@ struct MmaCons {
     }
     template <int ILP>
     __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int,
-                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                             int lane) {
+                                             const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                             uint32_t soff, const uint32_t *lut_l, int lane) {
         const int qtot = (m.cols + 3) >> 2;
         const int q0 = seg0 * m.seg_quads;
         const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
@@ -747,19 +846,18 @@ struct MmaCons {
             xcur = 0;
             load_window(xr, xrow, xok, colbase, 0, npieces);
         }
-        uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
-        const uint32_t kend = rows_now[0] * 32 + lane;
+        SegStream S(sm, soff, rows_now[0], lane);
         // pieces in pairs: piece p = 2 * pair (+1); a window holds 2 pairs
         for (int p = 0; p < npieces; p += 2) {
             uint32_t w[8];
             const int qc = 8 * p;
             if (qc + 8 <= nq) {
 #pragma unroll
-                for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P);
+                for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
             } else {
 #pragma unroll
                 for (int j = 0; j < 8; j++)
-                    w[j] = (qc + j < nq) ? q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P) : 0u;
+                    w[j] = (qc + j < nq) ? q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P) : 0u;
             }
             // the previous pair of MMAs is done with the A tile (and, at a window start, with the x tile)
             wait_mma(L);
@@ -791,18 +889,18 @@ struct MmaCons {
                 const int qc2 = qc + 8;
                 if (qc2 + 8 <= nq) {
 #pragma unroll
-                    for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P);
+                    for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 8; j++)
-                        w[j] = (qc2 + j < nq) ? q8_step_t<kWideLut>(lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P) : 0u;
+                        w[j] = (qc2 + j < nq) ? q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P) : 0u;
                 }
                 tmem_st_32x32b_x8_nowait(st_addr + 8u, w);
             }
             tmem_wait_st();
             issue(pw, two);
         }
-        if (hi != 0 || lo != P) atomicOr(L.status, MV_DEV_FINAL_STATE);
+        if (!S.ok()) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
     __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
                                                 int W, void *) {
@@ -856,16 +954,15 @@ __device__ __forceinline__ void i8x4_to_bf16x4(uint32_t wq, uint32_t &lo, uint32
 
 // Decode one 8-quad piece of the lane's row (zeros past nq).
 template <bool kWide>
-__device__ __forceinline__ void decode_piece(int qc, int nq, uint32_t &lo, uint32_t &hi, uint32_t &k, uint32_t kend,
-                                             const uint32_t *sb, const uint32_t *lut_l, uint32_t stride, int lane,
-                                             uint32_t &P, uint32_t (&w)[8]) {
+__device__ __forceinline__ void decode_piece(int qc, int nq, SegStream &S, const unsigned char *sm,
+                                             const uint32_t *lut_l, uint32_t stride, int lane, uint32_t (&w)[8]) {
     if (qc + 8 <= nq) {
 #pragma unroll
-        for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWide>(lo, hi, k, kend, sb, lut_l, stride, lane, P);
+        for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWide>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, stride, lane, S.P);
     } else {
 #pragma unroll
         for (int j = 0; j < 8; j++)
-            w[j] = (qc + j < nq) ? q8_step_t<kWide>(lo, hi, k, kend, sb, lut_l, stride, lane, P) : 0u;
+            w[j] = (qc + j < nq) ? q8_step_t<kWide>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, stride, lane, S.P) : 0u;
     }
 }
 
@@ -881,6 +978,8 @@ __device__ __forceinline__ void decode_piece(int qc, int nq, uint32_t &lo, uint3
 struct FwdMma {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;
+    static constexpr int kRedBufs = 1;
+    static constexpr bool kFinishSyncs = true;
     static constexpr int kMinCtas = 2;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
@@ -944,8 +1043,8 @@ struct FwdMma {
     }
     template <int ILP>
     __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int,
-                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                             int lane) {
+                                             const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                             uint32_t soff, const uint32_t *lut_l, int lane) {
         const int qtot = (m.cols + 3) >> 2;
         const int q0 = seg0 * m.seg_quads;
         const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
@@ -959,11 +1058,10 @@ struct FwdMma {
         const uint32_t xdst = xt + (uint32_t)hh * 512u + (uint32_t)(b >> 3) * 256u + (uint32_t)(b & 7) * 16u;
         uint4 xr[2 * kXPieces];
         load_window(xr, xrow, xok, colbase, 0, npieces);
-        uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
-        const uint32_t kend = rows_now[0] * 32 + lane;
+        SegStream S(sm, soff, rows_now[0], lane);
         for (int p = 0; p < npieces; p++) {
             uint32_t w[8];
-            decode_piece<kWideLut>(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P, w);
+            decode_piece<kWideLut>(8 * p, nq, S, sm, lut_l, L.lut_stride, lane, w);
             uint32_t a[16];
 #pragma unroll
             for (int j = 0; j < 8; j++) i8x4_to_bf16x4(w[j], a[2 * j], a[2 * j + 1]);
@@ -1003,7 +1101,7 @@ struct FwdMma {
             any = true;
             ncommit++;
         }
-        if (hi != 0 || lo != P) atomicOr(L.status, MV_DEV_FINAL_STATE);
+        if (!S.ok()) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
     __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
                                                 int W, void *) {
@@ -1054,6 +1152,8 @@ struct FwdMma {
 struct BwdMma {
     static constexpr int kNV = 32;
     static constexpr int kRedNV = 0;
+    static constexpr int kRedBufs = 1;
+    static constexpr bool kFinishSyncs = true;
     static constexpr int kMinCtas = 2;
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
@@ -1141,21 +1241,20 @@ struct BwdMma {
     }
     template <int ILP>
     __device__ __forceinline__ void run_step(const Q8SLaunch &L, const mv_q8_view &m, int seg0, int,
-                                             const uint32_t (&rows_now)[ILP], uint32_t *sb, const uint32_t *lut_l,
-                                             int lane) {
+                                             const uint32_t (&rows_now)[ILP], const unsigned char *sm,
+                                             uint32_t soff, const uint32_t *lut_l, int lane) {
         const int qtot = (m.cols + 3) >> 2;
         const int q0 = seg0 * m.seg_quads;
         const int nq = rows_now[0] ? min(m.seg_quads, qtot - q0) : 0;
         if (nq <= 0) return;
         const int npieces = (nq + 7) >> 3;
-        uint32_t lo = sb[lane], hi = sb[32 + lane], k = 64 + lane, P = 0;
-        const uint32_t kend = rows_now[0] * 32 + lane;
+        SegStream S(sm, soff, rows_now[0], lane);
         // lane = stripe row r: K step r / 16, K group (r / 8) % 2 (128 B), row r % 8 (16 B); N group g at 256 B
         const uint32_t wdst = wt + (uint32_t)(lane >> 4) * 1024u + (uint32_t)((lane >> 3) & 1) * 128u +
                               (uint32_t)(lane & 7) * 16u;
         for (int p = 0; p < npieces; p++) {
             uint32_t w[8];
-            decode_piece<kWideLut>(8 * p, nq, lo, hi, k, kend, sb, lut_l, L.lut_stride, lane, P, w);
+            decode_piece<kWideLut>(8 * p, nq, S, sm, lut_l, L.lut_stride, lane, w);
             uint32_t a[16];
 #pragma unroll
             for (int j = 0; j < 8; j++) i8x4_to_bf16x4(w[j], a[2 * j], a[2 * j + 1]);
@@ -1184,7 +1283,7 @@ struct BwdMma {
             pending = true;
             pend_col = 4 * q0 + 32 * p;
         }
-        if (hi != 0 || lo != P) atomicOr(L.status, MV_DEV_FINAL_STATE);
+        if (!S.ok()) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
     __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &, int, int, int lane, int, void *) {
         if (pending) flush(L, lane);
@@ -1218,6 +1317,206 @@ __global__ void q8s_chain_reset(Q8Job *jobs, int njobs) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x) jobs[j].pad = 0;
 }
 
+// Shared-memory layout of q8s_kernel (byte offsets), computed on the host and passed with the launch.
+__host__ __device__ inline Q8SLayout q8s_layout(uint32_t lut_bytes, uint32_t extra_bytes, uint32_t tbl_alias, int W,
+                                                int DEPTH, int ILP, int buf_words, int red_nv, int red_bufs,
+                                                int tbl_stage) {
+    Q8SLayout o{};
+    uint32_t p = lut_bytes;
+    o.extra = p;
+    p += extra_bytes;
+    o.bufs = p;  // [W][DEPTH][ILP][buf_words] u32 stream slots (128-byte multiples)
+    p += (uint32_t)(W * DEPTH * ILP) * (uint32_t)buf_words * 4u;
+    o.red = p;  // [red_bufs][W][red_nv][32] int
+    p += (uint32_t)(red_bufs * W * red_nv * 32) * 4u;
+    o.bars = p;  // [W][DEPTH] mbarriers
+    p += (uint32_t)(W * DEPTH) * 8u;
+    p = (p + 15u) & ~15u;
+    o.ring = p;
+    p += (uint32_t)kRing * (uint32_t)sizeof(ItemRec);
+    o.curs = p;  // [W] copy cursors (lane 0 of each warp)
+    p += (uint32_t)W * (uint32_t)sizeof(StepCursor);
+    o.sched = p;  // scheduler state (thread 0)
+    p += (uint32_t)sizeof(SchedState);
+    p = (p + 15u) & ~15u;
+    o.stage_o = p;  // [2][kStageOffs]
+    p += 2u * kStageOffs * 4u;
+    o.rows = p;  // [W][DEPTH][ILP] word-rows of each slot's blocks
+    p += (uint32_t)(W * DEPTH * ILP) * 4u;
+    p = (p + 15u) & ~15u;
+    // table staging: two areas (one item ahead), or one inside the consumer's region when that is free at
+    // table rebuilds and large enough (staged synchronously then)
+    const uint32_t stage_bytes = ((uint32_t)tbl_stage + kStagePad) * 2u;
+    if (tbl_alias >= stage_bytes) {
+        o.stage_e = o.extra;
+    } else {
+        o.stage_e = p;
+        p += 2u * stage_bytes;
+    }
+    o.total = p;
+    return o;
+}
+
+// Lane 0: issue copies while the warp has free slots and its cursor is on a visible step.
+template <int ILP, int DEPTH>
+__device__ __forceinline__ void pump_copies(const Q8SLaunch &L, StepCursor *cp, const ItemRec *ring, int kvis,
+                                            int warp, int W, uint32_t &issued, uint32_t consumed, unsigned char *sm,
+                                            uint32_t my_slots, uint32_t slot_bytes, uint64_t *my_bars,
+                                            uint32_t *my_rows) {
+    if (issued - consumed >= (uint32_t)DEPTH) return;
+    StepCursor c = *cp;
+    while (issued - consumed < (uint32_t)DEPTH && cursor_ready(c, ring, kvis, warp, W, ILP)) {
+        const int s = (int)(issued % DEPTH);
+        issue_step<ILP>(L, c, warp, W, sm, my_slots + (uint32_t)s * slot_bytes, &my_bars[s], my_rows + s * ILP);
+        issued++;
+        c.j++;
+    }
+    *cp = c;
+}
+
+// The table data of one item staged by the whole CTA from device memory (the first item, and consumers whose
+// staging area lies in their own region): offsets relative to the first entry in so[0..nt], entries from se[0].
+__device__ __forceinline__ void stage_table_sync(const Q8SLaunch &L, const mv_q8_view &m, int stripe, uint32_t *so,
+                                                 uint16_t *se) {
+    const uint32_t r0 = m.local ? (uint32_t)stripe * 32 : 0;
+    const uint32_t nt = m.local ? 32 : 1;
+    const uint32_t tb = __ldg(m.tbl_off + r0), te = __ldg(m.tbl_off + r0 + nt);
+    const bool ok = te >= tb && te <= m.tbl_len && te - tb <= (uint32_t)L.tbl_stage;
+    for (uint32_t i = threadIdx.x; i <= nt; i += blockDim.x) {
+        const uint32_t o = __ldg(m.tbl_off + r0 + i);
+        so[i] = (ok && o >= tb && o <= te) ? o - tb : 0;
+    }
+    if (threadIdx.x == 0) {
+        so[36] = ok;
+        so[37] = 0;
+        if (!ok) atomicOr(L.status, MV_DEV_BAD_TABLE);
+    }
+    const uint32_t n = ok ? te - tb : 0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) se[i] = __ldg(m.tbl + tb + i);
+}
+
+// Warp 0, staging the next item's table data while the current item decodes.  Phase 1: asynchronous copies
+// of its nt + 1 table offsets into so[0..nt].  Phase 2 (after the warp's first decode step): they give the
+// entry range, which 4-byte asynchronous copies (zero-filled past the readable end) bring in from an even entry
+// on; the offsets are rewritten relative to the first entry, so[36] = valid, so[37] = where the first entry
+// landed.  The copies complete before the barrier that ends the item (cp_async_wait_all).
+__device__ __forceinline__ void stage_offsets_async(const mv_q8_view &mn, int stripe, int lane, uint32_t *so) {
+    const uint32_t r0 = mn.local ? (uint32_t)stripe * 32u : 0u;
+    const uint32_t nt = mn.local ? 32u : 1u;
+    if ((uint32_t)lane <= nt) cp_async_4(so + lane, mn.tbl_off + r0 + lane, 4u);
+    if (lane == 0 && nt == 32u) cp_async_4(so + 32, mn.tbl_off + r0 + 32, 4u);
+    cp_async_commit();
+}
+__device__ __forceinline__ void stage_entries_async(const Q8SLaunch &L, const mv_q8_view &mn, int lane, uint32_t *so,
+                                                    uint16_t *se) {
+    cp_async_wait_all();
+    __syncwarp();
+    const uint32_t nt = mn.local ? 32u : 1u;
+    const uint32_t o = (uint32_t)lane <= nt ? so[lane] : 0u;
+    const uint32_t o32 = nt == 32u ? so[32] : 0u;
+    const uint32_t tb = so[0], te = so[nt];
+    __syncwarp();
+    const bool ok = te >= tb && te <= mn.tbl_len && te - tb <= (uint32_t)L.tbl_stage;
+    if ((uint32_t)lane <= nt) so[lane] = (ok && o >= tb && o <= te) ? o - tb : 0u;
+    if (lane == 0) {
+        if (nt == 32u) so[32] = (ok && o32 >= tb && o32 <= te) ? o32 - tb : 0u;
+        so[36] = ok;
+        so[37] = tb & 1u;
+    }
+    if (!ok) return;
+    const uint32_t a = tb & ~1u;
+    const uint32_t nch = (te - a + 1) >> 1;  // 4-byte pieces covering entries [a, te)
+    if (((uintptr_t)mn.tbl & 3) == 0) {
+        for (uint32_t c = lane; c < nch; c += 32) {
+            const uint32_t e = a + 2 * c;
+            const uint32_t avail = e < mn.tbl_len ? min(2u, mn.tbl_len - e) : 0u;
+            cp_async_4(se + 2 * c, mn.tbl + e, avail * 2u);
+        }
+        cp_async_commit();
+    } else {  // a table array that is not 4-byte aligned: plain loads
+        for (uint32_t c = lane; c < nch; c += 32) {
+            const uint32_t e = a + 2 * c;
+            se[2 * c] = e < mn.tbl_len ? __ldg(mn.tbl + e) : (uint16_t)0;
+            se[2 * c + 1] = e + 1 < mn.tbl_len ? __ldg(mn.tbl + e + 1) : (uint16_t)0;
+        }
+    }
+}
+
+// Decode table of one item from its staged data (so: relative offsets of the nt + 1 table bounds, tsm: the
+// entries u16 symbol | freq << 8).  Warp w fills quantiles [256 w / W, 256 (w + 1) / W) of every lane column.
+template <bool kWide>
+__device__ __forceinline__ void build_table(const Q8SLaunch &L, const mv_q8_view &m, uint32_t *lut,
+                                            const uint32_t *so, const uint16_t *tsm, int warp, int lane, int W) {
+    const int t = m.local ? lane : 0;
+    const uint32_t o0 = so[t], o1 = max(so[t + 1], o0);
+    const int qlo = (256 * warp) / W, qhi = (256 * (warp + 1)) / W;
+    uint32_t cum = 0;
+    if (kWide && !m.local) {
+        // one table for every row: lane j finds the entry of quantile qlo + j (the lanes walk the symbols
+        // together, without divergence) and writes it to all 32 lane columns, rotating the column so that a
+        // half-warp's stores hit distinct banks
+        uint2 *lut2 = reinterpret_cast<uint2 *>(lut);
+        bool bad = false;
+        for (uint32_t q0 = (uint32_t)qlo; q0 < (uint32_t)qhi; q0 += 32) {
+            const uint32_t q = q0 + lane, qend = min(q0 + 32, (uint32_t)qhi);
+            uint32_t c = 0, ent_q = 0, cum_q = 0;
+            bool found = false;
+            for (uint32_t k = o0; k < o1 && c < qend; k++) {
+                const uint32_t ent = tsm[k], f = ent >> 8;
+                if (!found && q < c + f) {  // q >= c: no earlier symbol contains q
+                    ent_q = ent;
+                    cum_q = c;
+                    found = true;
+                }
+                c += f;
+            }
+            if (q < qend) {
+                bad |= !found;
+                const uint2 v = found ? make_uint2((ent_q >> 8) | ((ent_q & 0xFFu) << 16), q - cum_q)
+                                      : make_uint2(1u, 0u);
+#pragma unroll 8
+                for (uint32_t i = 0; i < 32; i++) lut2[q * 32 + ((lane + i) & 31)] = v;
+            }
+        }
+        if (bad) atomicOr(L.status, MV_DEV_BAD_TABLE);
+        return;
+    }
+    uint32_t k = o0;
+    if (kWide && cum < (uint32_t)qlo) {
+        // symbols that end at or before qlo: one load, shift and add each (measured: 0.8 % faster for
+        // the CUDA-core consumers, 0.6 % slower for the tensor-core one, which keeps the plain loop)
+        uint32_t f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+        while (k < o1 && cum + f <= (uint32_t)qlo) {
+            cum += f;
+            k++;
+            f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+        }
+    }
+    for (; k < o1 && cum < (uint32_t)qhi; k++) {
+        const uint32_t ent = tsm[k];
+        const uint32_t f = ent >> 8, sym = ent & 0xFF;
+        const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
+        if constexpr (kWide) {
+            for (uint32_t q = a; q < e; q++)
+                reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(f | (sym << 16), q - cum);
+        } else {
+            // unrolled: measured 1 % faster for the tensor-core consumer (0.4 % slower for the wide table)
+#pragma unroll 4
+            for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
+        }
+        cum += f;
+    }
+    if (cum < (uint32_t)qhi) {
+        for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) {
+            if constexpr (kWide)
+                reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(1u, 0u);
+            else
+                lut[q * 32 + lane] = 1u;
+        }
+        atomicOr(L.status, MV_DEV_BAD_TABLE);
+    }
+}
+
 template <class Cons, int ILP, int DEPTH>
 __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(const Q8SLaunch L) {
     constexpr int NV = Cons::kRedNV;
@@ -1225,23 +1524,18 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = blockDim.x >> 5;
 
-    // decode table at the start of shared memory: 256 quantiles x 32 lanes of 4 B (narrow) or 8 B (wide)
-    constexpr int kLutBytes = Cons::kWideLut ? 256 * 32 * 8 : 256 * 32 * 4;
+    // decode table at the start of shared memory: 256 quantiles x 32 lanes of 4 B (narrow) or 8 B (wide); the
+    // rest of the layout comes with the launch (L.lay), so its offsets are constant-bank operands.
+    // Two staging areas: the next item's table data is staged while the current item decodes.
+    const bool async_tbl = L.lay.stage_e != L.lay.extra;
     uint32_t *lut = reinterpret_cast<uint32_t *>(smem);
-    unsigned char *extra = smem + kLutBytes;                                             // consumer region
-    uint32_t *bufs = reinterpret_cast<uint32_t *>(extra + Cons::extra_bytes(W));         // [W][DEPTH][ILP][buf]
-    int *red = reinterpret_cast<int *>(bufs + (size_t)W * DEPTH * ILP * L.buf_words);    // [W][NV][32]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(red + W * NV * 32);                    // [W][DEPTH]
-    uint32_t *toff_s = reinterpret_cast<uint32_t *>(bars + W * DEPTH);                   // [36]
-    uint32_t *rows_s = toff_s + 36;                                                      // [W][DEPTH][ILP]
-    // [tbl_stage]: its own region, or the consumer's area when that is free at table rebuilds and large enough
-    uint16_t *tsm = (size_t)L.tbl_stage * 2 <= Cons::tbl_alias_bytes(W)
-                        ? reinterpret_cast<uint16_t *>(extra)
-                        : reinterpret_cast<uint16_t *>(rows_s + W * DEPTH * ILP);
-
-    uint32_t *my_bufs = bufs + (size_t)warp * DEPTH * ILP * L.buf_words;
-    uint32_t *my_rows = rows_s + warp * DEPTH * ILP;
-    uint64_t *my_bars = bars + warp * DEPTH;
+    unsigned char *extra = smem + L.lay.extra;
+    ItemRec *ring = reinterpret_cast<ItemRec *>(smem + L.lay.ring);
+    StepCursor *my_cur = reinterpret_cast<StepCursor *>(smem + L.lay.curs) + warp;
+    SchedState *sch = reinterpret_cast<SchedState *>(smem + L.lay.sched);
+    const uint32_t my_slots = L.lay.bufs + (uint32_t)(warp * DEPTH) * L.slot_bytes;  // byte offset of slot 0
+    uint32_t *my_rows = reinterpret_cast<uint32_t *>(smem + L.lay.rows) + warp * DEPTH * ILP;
+    uint64_t *my_bars = reinterpret_cast<uint64_t *>(smem + L.lay.bars) + warp * DEPTH;
 
     // tensor-memory accumulators (MMA consumers): one warp allocates, all use, it frees at the end
     uint32_t tmem_base = 0;
@@ -1258,161 +1552,164 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
     if (lane == 0)
         for (int d = 0; d < DEPTH; d++) mbar_init(&my_bars[d], 1);
     fence_mbar_init();
-    __syncwarp();
 
-    // this warp's stream of (item, step) copies runs DEPTH steps ahead of its decode
-    StepCursor cur{};
-    uint32_t issued = 0;
-    if (lane == 0) {
-        cursor_seek(cur, L, blockIdx.x, warp, W, ILP);
-        for (int d = 0; d < DEPTH && cur.it < L.nitems; d++) {
-            const int slot = issued % DEPTH;
-            issue_step<ILP>(L, cur, warp, W, my_bufs + slot * ILP * L.buf_words, &my_bars[slot],
-                            my_rows + slot * ILP);
-            issued++;
-            if (++cur.j >= cur.steps) cursor_seek(cur, L, cur.it + gridDim.x, warp, W, ILP);
+    // scheduler (thread 0): the CTA's first two items
+    if (threadIdx.x == 0) {
+        SchedState st{};
+        for (int k = 0; k < 2; k++) {
+            ItemRec r{};
+            r.it = -1;
+            if (!st.grab_done) {
+                const uint32_t v = sched_grab(L, st.ngrab++);
+                sched_after_grab(L, v);
+                r = make_item(L, v, st.jhint);
+                st.grab_done = r.it < 0;
+            }
+            ring[k] = r;
         }
+        *sch = st;
     }
-    __syncwarp();
+    // this warp's copies run DEPTH steps ahead of its decode
+    if (lane == 0) {
+        StepCursor c{};
+        c.k = -1;
+        *my_cur = c;
+    }
+    __syncthreads();  // the first two ring entries, cursors and mbarrier inits are visible
+
+    uint32_t issued = 0, consumed = 0;
+    bool failed = false;  // a bounded wait ran out: no more copies or decodes (the status word has the flag)
+    if (lane == 0)
+        pump_copies<ILP, DEPTH>(L, my_cur, ring, 1, warp, W, issued, consumed, smem, my_slots, L.slot_bytes, my_bars,
+                                my_rows);
+    issued = __shfl_sync(0xffffffffu, issued, 0);  // lane 0 counts the copies; every lane tests them
 
     int lut_job = -1, lut_stripe = -1;
-    uint32_t consumed = 0;
+    int pf_state = 0;  // warp 0: 0 nothing to stage, 1 offsets in flight, 2 entries in flight
     const uint32_t *lut_l = Cons::kWideLut ? lut : lut + lane;  // wide steps add the lane themselves
-    for (uint32_t it = blockIdx.x; it < L.nitems; it += gridDim.x) {
-        const ItemInfo I = find_item(L, it);
+    for (int k = 0;; k++) {
+        const ItemRec I = ring[k % kRing];
+        if (I.it < 0) break;
         const Q8Job &J = job_at(L, I.job);
         const mv_q8_view &m = J.m;
-        int sbeg, send;
-        item_segs(m, J.ngroups, I.group, sbeg, send);
+        const uint32_t area = async_tbl ? (uint32_t)(k & 1) : 0u;
 
-        // decode table, rebuilt only when it changes (uniform across the CTA)
+        // decode table, rebuilt only when it changes (uniform across the CTA).  Every warp finished the
+        // previous item's decode before the CTA barrier that ended it.
         if (I.job != lut_job || (m.local && I.stripe != lut_stripe)) {
-            __syncthreads();  // every warp is done with the previous table
-            const uint32_t r0 = m.local ? (uint32_t)I.stripe * 32 : 0;
-            const uint32_t nt = m.local ? 32 : 1;
-            const uint32_t tb = __ldg(m.tbl_off + r0), te = __ldg(m.tbl_off + r0 + nt);
-            const bool ok = te >= tb && te <= m.tbl_len && te - tb <= (uint32_t)L.tbl_stage;
-            for (uint32_t i = threadIdx.x; i <= nt; i += blockDim.x) {
-                const uint32_t o = __ldg(m.tbl_off + r0 + i);
-                toff_s[i] = (ok && o >= tb && o <= te) ? o - tb : 0;
-            }
-            if (!ok && threadIdx.x == 0) atomicOr(L.status, MV_DEV_BAD_TABLE);
-            const uint32_t n = ok ? te - tb : 0;
-            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) tsm[i] = __ldg(m.tbl + tb + i);
-            __syncthreads();
-            const int t = m.local ? lane : 0;
-            const uint32_t o0 = toff_s[t], o1 = max(toff_s[t + 1], o0);
-            const int qlo = (256 * warp) / W, qhi = (256 * (warp + 1)) / W;
-            uint32_t cum = 0;
-            if (Cons::kWideLut && !m.local) {
-                // one table for every row: lane j finds the entry of quantile qlo + j (the lanes walk the symbols
-                // together, without divergence) and writes it to all 32 lane columns, rotating the column so
-                // that a half-warp's stores hit distinct banks
-                uint2 *lut2 = reinterpret_cast<uint2 *>(lut);
-                bool bad = false;
-                for (uint32_t q0 = (uint32_t)qlo; q0 < (uint32_t)qhi; q0 += 32) {
-                    const uint32_t q = q0 + lane, qend = min(q0 + 32, (uint32_t)qhi);
-                    uint32_t c = 0, ent_q = 0, cum_q = 0;
-                    bool found = false;
-                    for (uint32_t k = o0; k < o1 && c < qend; k++) {
-                        const uint32_t ent = tsm[k], f = ent >> 8;
-                        if (!found && q < c + f) {  // q >= c: no earlier symbol contains q
-                            ent_q = ent;
-                            cum_q = c;
-                            found = true;
-                        }
-                        c += f;
-                    }
-                    if (q < qend) {
-                        bad |= !found;
-                        const uint2 v = found ? make_uint2((ent_q >> 8) | ((ent_q & 0xFFu) << 16), q - cum_q)
-                                              : make_uint2(1u, 0u);
-#pragma unroll 8
-                        for (uint32_t i = 0; i < 32; i++) lut2[q * 32 + ((lane + i) & 31)] = v;
-                    }
-                }
-                if (bad) atomicOr(L.status, MV_DEV_BAD_TABLE);
-                cum = (uint32_t)qhi;  // done: the per-lane loops below do nothing
-            }
-            uint32_t k = o0;
-            if (Cons::kWideLut && cum < (uint32_t)qlo) {
-                // symbols that end at or before qlo: one load, shift and add each (measured: 0.8 % faster for
-                // the CUDA-core consumers, 0.6 % slower for the tensor-core one, which keeps the plain loop)
-                uint32_t f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
-                while (k < o1 && cum + f <= (uint32_t)qlo) {
-                    cum += f;
-                    k++;
-                    f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
-                }
-            }
-            for (; k < o1 && cum < (uint32_t)qhi; k++) {
-                const uint32_t ent = tsm[k];
-                const uint32_t f = ent >> 8, sym = ent & 0xFF;
-                const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
-                if constexpr (Cons::kWideLut) {
-                    for (uint32_t q = a; q < e; q++)
-                        reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(f | (sym << 16), q - cum);
-                } else {
-                    // unrolled: measured 1 % faster for the tensor-core consumer (0.4 % slower for the wide table)
-#pragma unroll 4
-                    for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
-                }
-                cum += f;
-            }
-            if (cum < (uint32_t)qhi) {
-                for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) {
-                    if constexpr (Cons::kWideLut)
-                        reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(1u, 0u);
-                    else
-                        lut[q * 32 + lane] = 1u;
-                }
+            uint32_t *so = reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + area * kStageOffs;
+            uint16_t *se = reinterpret_cast<uint16_t *>(smem + L.lay.stage_e) + area * L.stage_len;
+            if (!async_tbl || k == 0) {
+                __syncthreads();  // the staging area may be the consumer's region
+                stage_table_sync(L, m, I.stripe, so, se);
+                __syncthreads();
+            } else if (threadIdx.x == 0 && so[36] == 0) {
                 atomicOr(L.status, MV_DEV_BAD_TABLE);
             }
+            build_table<Cons::kWideLut>(L, m, lut, so, se + so[37], warp, lane, W);
             fence_proxy_async_smem();  // the table staging may share memory with later bulk copies
             __syncthreads();
             lut_job = I.job;
             lut_stripe = I.stripe;
         }
 
+        // thread 0: take the CTA's item k + 2 now and record it at the end of this item (the atomic's
+        // latency overlaps the decode)
+        if (threadIdx.x == 0) {
+            sch->grab_now = 0;
+            if (!sch->grab_done) {
+                sch->pending = sched_grab(L, sch->ngrab++);
+                sch->grab_now = 1;
+            }
+        }
+        // warp 0, first phase of staging the next item's table data: its offsets
+        pf_state = 0;
+        if (async_tbl && warp == 0) {
+            const ItemRec &N = ring[(k + 1) % kRing];
+            if (N.it >= 0) {
+                const mv_q8_view &mn = job_at(L, N.job).m;
+                if (N.job != I.job || (mn.local && N.stripe != I.stripe)) {
+                    stage_offsets_async(mn, N.stripe, lane,
+                                        reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + (area ^ 1u) * kStageOffs);
+                    pf_state = 1;
+                }
+            }
+        }
+
         if (L.chain_scales && I.job > 0) chain_wait(L, I.job - 1);
         cons.begin_item(L, J, I.stripe, lane, I.job);
-        const int steps = warp_steps(send - sbeg, warp, W, ILP);
+        // ring[k + 1] was recorded during item k - 1 (or before the first item) and is visible now
+        const int kvis = k + 1;
+        if (lane == 0 && !failed)
+            pump_copies<ILP, DEPTH>(L, my_cur, ring, kvis, warp, W, issued, consumed, smem, my_slots, L.slot_bytes,
+                                    my_bars, my_rows);
+        issued = __shfl_sync(0xffffffffu, issued, 0);
+        const int steps = warp_steps(I.se - I.sb, warp, W, ILP);
         for (int j = 0; j < steps; j++) {
             const int slot = consumed % DEPTH;
             const uint32_t parity = (consumed / DEPTH) & 1;
+            const bool was_issued = consumed < issued;
             uint32_t rows_now[ILP];
             bool any = false;
 #pragma unroll
-            for (int k = 0; k < ILP; k++) {
-                rows_now[k] = my_rows[slot * ILP + k];
-                any |= rows_now[k] != 0;
+            for (int kk = 0; kk < ILP; kk++) {
+                rows_now[kk] = my_rows[slot * ILP + kk];
+                any |= rows_now[kk] != 0;
             }
-            if (any) {
-                if (mbar_wait_bounded(&my_bars[slot], parity, L.status, L.spin_limit)) {
-                    cons.template run_step<ILP>(L, m, sbeg + warp + j * W * ILP, W, rows_now,
-                                                my_bufs + slot * ILP * L.buf_words, lut_l, lane);
+            if (was_issued && any) {
+                if (!failed) {
+                    const bool ok =
+                        __all_sync(0xffffffffu, mbar_wait_bounded(&my_bars[slot], parity, L.status, L.spin_limit));
+                    if (ok) {
+                        cons.template run_step<ILP>(L, m, I.sb + warp + j * W * ILP, W, rows_now, smem,
+                                                    my_slots + (uint32_t)slot * L.slot_bytes, lut_l, lane);
+                    } else {
+                        failed = true;  // wait once more (bounded) so that no copy is left writing the slot
+                        mbar_wait_bounded(&my_bars[slot], parity, nullptr, L.spin_limit);
+                    }
                 } else {
-                    mbar_wait_bounded(&my_bars[slot], parity, nullptr, L.spin_limit);
+                    mbar_wait_bounded(&my_bars[slot], parity, nullptr, L.spin_limit);  // drain, no decode
                 }
             }
             __syncwarp();
             consumed++;
             // the slot is free: refill it with the step DEPTH ahead in this warp's stream
-            if (lane == 0 && cur.it < L.nitems) {
-                const int s2 = issued % DEPTH;
-                issue_step<ILP>(L, cur, warp, W, my_bufs + s2 * ILP * L.buf_words, &my_bars[s2], my_rows + s2 * ILP);
-                issued++;
-                if (++cur.j >= cur.steps) cursor_seek(cur, L, cur.it + gridDim.x, warp, W, ILP);
+            if (lane == 0 && !failed)
+                pump_copies<ILP, DEPTH>(L, my_cur, ring, kvis, warp, W, issued, consumed, smem, my_slots,
+                                        L.slot_bytes, my_bars, my_rows);
+            issued = __shfl_sync(0xffffffffu, issued, 0);
+            if (pf_state == 1) {  // warp 0, second phase (after its first step): the entries
+                stage_entries_async(L, job_at(L, ring[(k + 1) % kRing].job).m, lane,
+                                    reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + (area ^ 1u) * kStageOffs,
+                                    reinterpret_cast<uint16_t *>(smem + L.lay.stage_e) + (area ^ 1u) * L.stage_len);
+                pf_state = 2;
             }
-            __syncwarp();
+        }
+        if (pf_state == 1)
+            stage_entries_async(L, job_at(L, ring[(k + 1) % kRing].job).m, lane,
+                                reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + (area ^ 1u) * kStageOffs,
+                                reinterpret_cast<uint16_t *>(smem + L.lay.stage_e) + (area ^ 1u) * L.stage_len);
+        if (pf_state) cp_async_wait_all();  // visible to the CTA after the barrier that ends the item
+        if (threadIdx.x == 0 && sch->grab_now) {  // record item k + 2
+            SchedState st = *sch;
+            sched_after_grab(L, st.pending);
+            const ItemRec r = make_item(L, st.pending, st.jhint);
+            st.grab_done = r.it < 0;
+            *sch = st;
+            ring[(k + 2) % kRing] = r;
         }
 
-        cons.finish_item(L, J, I.stripe, warp, lane, W, red);  // ends with a CTA barrier
+        cons.finish_item(L, J, I.stripe, warp, lane, W,
+                         reinterpret_cast<int *>(smem + L.lay.red) + (Cons::kRedBufs == 2 ? (k & 1) : 0) * W * NV * 32);
+        if (!Cons::kFinishSyncs) __syncthreads();
         if (L.chain_scales && threadIdx.x == 0) {
             __threadfence();  // this item's outputs are visible before it is counted
             atomicAdd(const_cast<uint32_t *>(&L.jobs[I.job].pad), 1u);
         }
     }
+    // copies still in flight (only after a failed wait) land before the CTA exits
+    for (; consumed < issued; consumed++)
+        mbar_wait_bounded(&my_bars[consumed % DEPTH], (consumed / DEPTH) & 1, nullptr, L.spin_limit);
     if (Cons::kTmemCols) {
         cons.drain(L);
         tcgen05_fence_before();
@@ -1471,13 +1768,6 @@ __global__ void q8s_scale_atomic_y(const Q8Job *jobs, int njobs, int batch) {
 
 namespace {
 
-size_t q8s_smem(int NV, int ILP, int DEPTH, int W, int buf_words, int tbl_stage, size_t extra, size_t tbl_alias,
-                bool wide_lut) {
-    const size_t tbl = (size_t)tbl_stage * 2 <= tbl_alias ? 0 : (size_t)tbl_stage * 2;
-    return (size_t)256 * 32 * (wide_lut ? 8 : 4) + extra + (size_t)W * DEPTH * ILP * buf_words * 4 + (size_t)W * NV * 32 * 4 +
-           (size_t)W * DEPTH * 8 + 36 * 4 + (size_t)W * DEPTH * ILP * 4 + tbl;
-}
-
 mv_status resident_ctas(const void *kern, size_t smem, int threads, int *out) {
     int d = 0, smem_sm = 0, reserved = 0;
     MV_CUDA_TRY(cudaGetDevice(&d), "cudaGetDevice");
@@ -1494,15 +1784,20 @@ mv_status resident_ctas(const void *kern, size_t smem, int threads, int *out) {
 }
 
 template <class Cons, int ILP, int DEPTH>
-mv_status launch_q8s_t(const Q8SLaunch &L, int W, int ctas_per_sm, cudaStream_t st) {
+mv_status launch_q8s_t(const Q8SLaunch &L0, int W, int ctas_per_sm, cudaStream_t st) {
     if (32 * W > Cons::kMaxThreads)
         return fail(MV_ERR_ARG, "Q8 launch: %d warps per CTA; this engine takes at most %d", W,
                     Cons::kMaxThreads / 32);
     if (Cons::extra_bytes(W) % 16)  // the stream buffers behind the consumer region take bulk copies
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch: consumer region of %zu B breaks 16-byte alignment",
                     Cons::extra_bytes(W));
-    const size_t smem = q8s_smem(Cons::kRedNV, ILP, DEPTH, W, L.buf_words, L.tbl_stage, Cons::extra_bytes(W),
-                                 Cons::tbl_alias_bytes(W), Cons::kWideLut);
+    Q8SLaunch L = L0;
+    L.lay = q8s_layout(Cons::kWideLut ? 256 * 32 * 8 : 256 * 32 * 4, (uint32_t)Cons::extra_bytes(W),
+                       (uint32_t)Cons::tbl_alias_bytes(W), W, DEPTH, ILP, L.buf_words, Cons::kRedNV, Cons::kRedBufs,
+                       L.tbl_stage);
+    L.slot_bytes = (uint32_t)ILP * (uint32_t)L.buf_words * 4u;
+    L.stage_len = (uint32_t)L.tbl_stage + kStagePad;
+    const size_t smem = L.lay.total;
     if (smem > (size_t)max_smem_optin())
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch needs %zu B of shared memory (max %d)", smem,
                     max_smem_optin());
@@ -1616,6 +1911,7 @@ void plan_job(Q8Job &J, const mv_q8_tuning &t, uint32_t &item, int parts) {
     J.ngroups = std::max(1, std::min(parts > 0 ? parts : 1, J.m.nseg));
     J.atomic = J.ngroups > 1;
     J.item0 = item;
+    J.pad = 0;  // work-queue counter (job 0 of a stack) or item counter (chains)
     item += (uint32_t)((J.m.rows + 31) / 32) * (uint32_t)J.ngroups;
 }
 
@@ -1848,6 +2144,8 @@ mv_status mv_q8_stack_matvec(const mv_q8_job *jobs_dev, int njobs, const mv_q8_s
     L.buf_words = (info->max_blk_rows + 1) * 32;
     L.tbl_stage = (int)((info->tbl_stripe_max + 7) & ~7u);
     L.lut_stride = 32;
+    // work queue: jobs_dev[0].pad, zero after planning and after every completed launch
+    if (info->nitems < 0x7FFFFFFFu) L.queue = const_cast<uint32_t *>(&jobs_dev[0].pad);
     dim3 zg(64, std::min(njobs, 1024));
     if (info->atomic_jobs > 0) {
         mv::q8s_zero_atomic_y<<<zg, 256, 0, st>>>(jobs_dev, njobs, batch);

@@ -65,6 +65,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+// 4-byte asynchronous copy global -> shared (cp.async, no registers): src_bytes (0, 2 or 4) are read, the
+// rest of the 4 bytes is zero-filled.  dst and src 4-byte aligned.  Completion: cp_async_commit, then
+// cp_async_wait_all in the issuing thread (and a barrier for other threads).
+__device__ __forceinline__ void cp_async_4(void *dst, const void *src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ uint4 ldg_nc_u4(const uint4 *p) {
     uint4 v;
     asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
