@@ -380,6 +380,56 @@ mv_status mv_write_safetensors(const char *path, const mv_blob *b);
  * "m<i>.rows", "m<i>.cols", "m<i>.min_value", "m<i>.G", "m<i>.payload_size". */
 mv_status mv_read_wpr_bin(const char *path, mv_blob **out);
 
+/* ------------------------------------------------------------- Q8 files --- */
+
+/* Host arrays of one Q8 matrix (as mv_q8_encode returns them; see mv_q8_view
+ * for the layout) and, optionally, its per-row fp32 scales. */
+typedef struct mv_q8_host {
+    const uint32_t *blocks;   size_t n_blocks;   /* u32 words, a multiple of 32 */
+    const uint32_t *blk_off;  size_t n_blk_off;  /* stripes*nseg + 1            */
+    const uint16_t *tbl;      size_t n_tbl;
+    const uint32_t *tbl_off;  size_t n_tbl_off;  /* tables + 1                  */
+    int32_t rows, cols, seg_quads, nseg, local, max_blk_rows;
+    uint32_t tbl_stripe_max;
+    const float *row_scales;  /* [rows] or NULL */
+} mv_q8_host;
+
+/* The chained workload stored with a file (the reference's end-to-end
+ * pipeline, buffered/encoder.py:42-51), every field optional (NULL). */
+typedef struct mv_q8_chain_host {
+    const int8_t *initial_vector; size_t n_initial;
+    const float *scales;     /* [count] requantisation scale of each step */
+    const uint32_t *hashes;  /* [count] hash of each step's int8 output   */
+} mv_q8_chain_host;
+
+/* Writes `count` Q8 matrices (and the chain data, if given) as one safetensors
+ * file, in the convention of the reference's files (buffered/encoder.py:473-511:
+ * concatenated arrays with per-matrix start offsets; the chain tensors keep the
+ * reference's names initial_vector / scales / hashes).  Tensors: q8_meta I32
+ * [count, 8] (rows, cols, seg_quads, nseg, local, max_blk_rows, tbl_stripe_max,
+ * has_row_scales), q8_blocks/q8_blk_off/q8_tbl/q8_tbl_off and row_scales, each
+ * with a "<name>_start" U64 [count + 1].  Every matrix is checked against the
+ * layout's shape rules first (MV_ERR_FORMAT). */
+mv_status mv_q8_save(const char *path, const mv_q8_host *mats, int count, const mv_q8_chain_host *chain);
+
+/* Reading: a file opened with mv_read_safetensors holds `count` matrices;
+ * mv_q8_file_matrix fills `out` with pointers into the blob (valid until it is
+ * freed) after the same checks, mv_q8_file_chain the chain data (NULL fields
+ * when absent). */
+mv_status mv_q8_file_count(const mv_blob *file, int *count);
+mv_status mv_q8_file_matrix(const mv_blob *file, int index, mv_q8_host *out);
+mv_status mv_q8_file_chain(const mv_blob *file, mv_q8_chain_host *out);
+
+/* A Q8 matrix in device memory of the current device, owned by the handle
+ * (these calls allocate; the launch paths never do).  mv_q8_load reads matrix
+ * `index` of a file and uploads it; the view is valid until mv_q8_matrix_free. */
+typedef struct mv_q8_matrix mv_q8_matrix;
+mv_status mv_q8_upload(const mv_q8_host *h, mv_q8_matrix **out);
+mv_status mv_q8_load(const char *path, int index, mv_q8_matrix **out);
+const mv_q8_view *mv_q8_matrix_view(const mv_q8_matrix *m);
+const float *mv_q8_matrix_row_scales(const mv_q8_matrix *m);  /* device pointer or NULL */
+void mv_q8_matrix_free(mv_q8_matrix *m);
+
 /* Fault injection for tests of the device-side error paths (no reference
  * counterpart).  MV_INJECT_WAIT_LIMIT sets the iteration bound of every
  * shared-memory barrier wait (0 restores the default); MV_INJECT_DROP_COPY

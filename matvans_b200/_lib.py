@@ -26,7 +26,9 @@ EXPORTS = [
     "mv_hash_int8", "mv_debug_inject", "mv_requant_absmax_noalloc", "mv_q8_matvec_tuned", "mv_q8_stack_plan",
     "mv_q8_stack_matvec", "mv_q8_matvec_bf16", "mv_q8_matvec_t_bf16", "mv_q8_chain_plan", "mv_q8_chain_matvec",
     "mv_aws_matvec", "mv_aws_matvec_requant", "mv_aws_encode", "mat_vec_mul_coalesced_stripes",
-    "mv_q8_x_tiles_bytes", "mv_debug_query",
+    "mv_q8_x_tiles_bytes", "mv_debug_query", "mv_q8_save", "mv_q8_file_count", "mv_q8_file_matrix",
+    "mv_q8_file_chain", "mv_q8_upload", "mv_q8_load", "mv_q8_matrix_view", "mv_q8_matrix_row_scales",
+    "mv_q8_matrix_free",
 ]
 
 
@@ -43,6 +45,22 @@ class Q8View(ctypes.Structure):
                 ("seg_quads", ctypes.c_int32), ("nseg", ctypes.c_int32), ("local", ctypes.c_int32),
                 ("max_blk_rows", ctypes.c_int32), ("blocks_rows", ctypes.c_uint32),
                 ("tbl_len", ctypes.c_uint32), ("tbl_stripe_max", ctypes.c_uint32)]
+
+
+class Q8Host(ctypes.Structure):
+    """struct mv_q8_host."""
+    _fields_ = [("blocks", ctypes.c_void_p), ("n_blocks", ctypes.c_size_t), ("blk_off", ctypes.c_void_p),
+                ("n_blk_off", ctypes.c_size_t), ("tbl", ctypes.c_void_p), ("n_tbl", ctypes.c_size_t),
+                ("tbl_off", ctypes.c_void_p), ("n_tbl_off", ctypes.c_size_t), ("rows", ctypes.c_int32),
+                ("cols", ctypes.c_int32), ("seg_quads", ctypes.c_int32), ("nseg", ctypes.c_int32),
+                ("local", ctypes.c_int32), ("max_blk_rows", ctypes.c_int32), ("tbl_stripe_max", ctypes.c_uint32),
+                ("row_scales", ctypes.c_void_p)]
+
+
+class Q8ChainHost(ctypes.Structure):
+    """struct mv_q8_chain_host."""
+    _fields_ = [("initial_vector", ctypes.c_void_p), ("n_initial", ctypes.c_size_t), ("scales", ctypes.c_void_p),
+                ("hashes", ctypes.c_void_p)]
 
 
 class Q8Tuning(ctypes.Structure):
@@ -115,6 +133,15 @@ def lib():
         "mv_hash_int8": ([P, sz], ctypes.c_uint32),
         "mv_debug_inject": ([i32, ctypes.c_uint32], st),
         "mv_debug_query": ([i32, ctypes.POINTER(ctypes.c_uint64)], st),
+        "mv_q8_save": ([ctypes.c_char_p, ctypes.POINTER(Q8Host), i32, ctypes.POINTER(Q8ChainHost)], st),
+        "mv_q8_file_count": ([P, ctypes.POINTER(i32)], st),
+        "mv_q8_file_matrix": ([P, i32, ctypes.POINTER(Q8Host)], st),
+        "mv_q8_file_chain": ([P, ctypes.POINTER(Q8ChainHost)], st),
+        "mv_q8_upload": ([ctypes.POINTER(Q8Host), ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_q8_load": ([ctypes.c_char_p, i32, ctypes.POINTER(ctypes.c_void_p)], st),
+        "mv_q8_matrix_view": ([P], ctypes.POINTER(Q8View)),
+        "mv_q8_matrix_row_scales": ([P], P),
+        "mv_q8_matrix_free": ([P], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

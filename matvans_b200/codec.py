@@ -337,6 +337,79 @@ def q8_encode(matrix, local=True, seg_quads=0, nthreads=0):
     return out
 
 
+_Q8_KEYS = ("rows", "cols", "seg_quads", "nseg", "local", "max_blk_rows", "tbl_stripe_max")
+
+
+def save_q8(path, encodings, row_scales=None, chain=None):
+    """Write Q8 encodings (dicts from q8_encode) as one safetensors file (mv_q8_save).  row_scales: optional
+    list of per-row fp32 arrays (None entries allowed); chain: optional dict with "initial_vector" (int8),
+    "scales" (fp32 per matrix) and "hashes" (u32 per matrix), stored under the reference's tensor names."""
+    keep, hosts = [], (_lib.Q8Host * len(encodings))()
+    for i, e in enumerate(encodings):
+        arrs = [np.ascontiguousarray(e["blocks"], np.uint32), np.ascontiguousarray(e["blk_off"], np.uint32),
+                np.ascontiguousarray(e["tbl"], np.uint16), np.ascontiguousarray(e["tbl_off"], np.uint32)]
+        sc = None if row_scales is None or row_scales[i] is None else np.ascontiguousarray(row_scales[i], np.float32)
+        if sc is not None and sc.shape != (int(e["rows"]),):
+            raise ValueError(f"row_scales[{i}] must have {e['rows']} entries")
+        keep += arrs + ([sc] if sc is not None else [])
+        h = hosts[i]
+        h.blocks, h.blk_off, h.tbl, h.tbl_off = [a.ctypes.data for a in arrs]
+        h.n_blocks, h.n_blk_off, h.n_tbl, h.n_tbl_off = [a.size for a in arrs]
+        for k in _Q8_KEYS:
+            setattr(h, k, int(e[k]))
+        h.row_scales = sc.ctypes.data if sc is not None else None
+    ch = None
+    if chain:
+        ch = _lib.Q8ChainHost()
+        for k, dt in (("initial_vector", np.int8), ("scales", np.float32), ("hashes", np.uint32)):
+            if chain.get(k) is not None:
+                a = np.ascontiguousarray(chain[k], dt)
+                if k != "initial_vector" and a.size != len(encodings):
+                    raise ValueError(f"chain {k} needs one entry per matrix")
+                keep.append(a)
+                setattr(ch, k, a.ctypes.data)
+                if k == "initial_vector":
+                    ch.n_initial = a.size
+    check(lib().mv_q8_save(str(path).encode(), hosts, len(encodings), ctypes.byref(ch) if ch else None))
+
+
+def load_q8(path):
+    """Read a Q8 file written by save_q8 / mv_q8_save: (encodings, row_scales, chain).  encodings are dicts in
+    q8_encode's form (host arrays), row_scales a list of fp32 arrays or None, chain a dict (entries None when
+    absent).  The file is checked against the layout's shape rules (mv_q8_file_matrix)."""
+    h = _lib.new_blob_out()
+    check(lib().mv_read_safetensors(str(path).encode(), ctypes.byref(h)))
+    b = Blob(h.value)
+    n = ctypes.c_int32()
+    check(lib().mv_q8_file_count(b._h, ctypes.byref(n)))
+    encs, scales = [], []
+
+    def grab(p, cnt, dt):
+        if not p or not cnt:
+            return np.zeros(0, dt)
+        buf = (ctypes.c_char * (cnt * np.dtype(dt).itemsize)).from_address(p)
+        return np.frombuffer(buf, dtype=dt).copy()
+    for i in range(n.value):
+        q = _lib.Q8Host()
+        check(lib().mv_q8_file_matrix(b._h, i, ctypes.byref(q)))
+        e = {k: int(getattr(q, k)) for k in _Q8_KEYS}
+        e["blocks"] = grab(q.blocks, q.n_blocks, np.uint32)
+        e["blk_off"] = grab(q.blk_off, q.n_blk_off, np.uint32)
+        e["tbl"] = grab(q.tbl, q.n_tbl, np.uint16)
+        e["tbl_off"] = grab(q.tbl_off, q.n_tbl_off, np.uint32)
+        e["payload_bytes"] = (4 * int(e["blk_off"][-1]) * 32 + 2 * e["tbl"].size + 4 * e["tbl_off"].size +
+                              4 * e["blk_off"].size)
+        e["bits_per_weight"] = 8.0 * e["payload_bytes"] / (e["rows"] * e["cols"])
+        encs.append(e)
+        scales.append(grab(q.row_scales, e["rows"], np.float32) if q.row_scales else None)
+    c = _lib.Q8ChainHost()
+    check(lib().mv_q8_file_chain(b._h, ctypes.byref(c)))
+    chain = {"initial_vector": grab(c.initial_vector, c.n_initial, np.int8) if c.initial_vector else None,
+             "scales": grab(c.scales, n.value, np.float32) if c.scales else None,
+             "hashes": grab(c.hashes, n.value, np.uint32) if c.hashes else None}
+    return encs, scales, chain
+
+
 __all__ = [n for n in dir() if not n.startswith("_")]
 if sys.byteorder != "little":  # pragma: no cover
     raise ImportError("matvans_b200 assumes a little-endian host, like the reference")

@@ -202,6 +202,17 @@ class Q8Matrix(_Matrix):
         from . import codec
         return cls(codec.q8_encode(W, local=local, seg_quads=seg_quads), device)
 
+    def to_encoding(self):
+        """The host form of this matrix (q8_encode's dict), e.g. for codec.save_q8."""
+        e = {"rows": self.rows, "cols": self.cols, "seg_quads": self.seg_quads, "nseg": self.nseg,
+             "local": self.local, "max_blk_rows": self.max_blk_rows, "tbl_stripe_max": self.tbl_stripe_max,
+             "payload_bytes": self.payload_bytes, "bits_per_weight": self.bits_per_weight}
+        e["blocks"] = self.blocks.cpu().numpy().view(np.uint32)
+        e["blk_off"] = self.blk_off.cpu().numpy().view(np.uint32)
+        e["tbl"] = self.tbl.cpu().numpy().view(np.uint16)
+        e["tbl_off"] = self.tbl_off.cpu().numpy().view(np.uint32)
+        return e
+
     def view(self):
         return Q8View(self.blocks.data_ptr(), self.blk_off.data_ptr(), self.tbl.data_ptr(),
                       self.tbl_off.data_ptr(), self.rows, self.cols, self.seg_quads, self.nseg, self.local,
@@ -251,6 +262,17 @@ class Q8Matrix(_Matrix):
         W = torch.empty((self.rows, self.cols), dtype=torch.int8, device=self.device)
         check(lib().mv_q8_decode(ctypes.byref(self._view), _p(W), _stream()))
         return W
+
+
+def load_q8(path, device="cuda"):
+    """Every matrix of a Q8 file (codec.save_q8 / mv_q8_save) on `device`: (matrices, row_scales, chain) with
+    row_scales a list of fp32 device tensors (None where the file has none) and chain the file's chain data
+    (host arrays, None when absent)."""
+    from . import codec
+    encs, scales, chain = codec.load_q8(path)
+    dev = torch.device(device)
+    mats = [Q8Matrix(e, dev) for e in encs]
+    return mats, [None if s is None else torch.from_numpy(s).to(dev) for s in scales], chain
 
 
 class Q8Stack:
