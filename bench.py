@@ -360,7 +360,7 @@ def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, r
                     raise SystemExit(f"bench: cuBLAS int8 GEMM disagrees with dense dp4a on {m['spec']['name']}")
         cands = autotune.candidates_for(B, autotune.CANDIDATES)
         best, res = autotune.tune_stack(lambda t: ops.Q8Stack(Ms, batch=B, tuning=t, xs=xs, device=dev),
-                                        candidates=cands, reps=reps)
+                                        candidates=cands, reps=reps, key=autotune.stack_key(Ms, B))
         row = {}
         engines = (0, 1) if B >= 8 else (0,)
         for eng in engines:
@@ -673,7 +673,8 @@ def run_ours(args):
         stack_tuning, stack_cands = tuple(int(v) for v in args.tuning.split(",")), {}
     else:
         stack_tuning, stack_cands = autotune.tune_stack(
-            lambda t: ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=t, xs=xs, device=dev))
+            lambda t: ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=t, xs=xs, device=dev),
+            key=autotune.stack_key([e["M"] for e in entries], 1))
     S = ops.Q8Stack([e["M"] for e in entries], batch=1, tuning=stack_tuning, xs=xs, device=dev)
     # correctness gate before timing: bit-exact against the host int64 matvec
     S.run()

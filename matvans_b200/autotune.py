@@ -24,7 +24,7 @@ from . import _lib
 from ._lib import Q8Tuning
 
 # (warps, ilp, depth, ctas_per_sm, parts, engine)
-CANDIDATES = [(w, ilp, d, 0, 0, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)]
+CANDIDATES = [(w, ilp, d, 0, 0, 0) for w in (4, 8, 16) for ilp in (1, 2) for d in (1, 2)]
 # single matrices additionally try splitting each stripe into more work items
 SINGLE_CANDIDATES = CANDIDATES + [(w, ilp, d, 0, p, 0) for w in (4, 8) for ilp in (1, 2) for d in (1, 2)
                                   for p in (2, 4)]
@@ -153,8 +153,27 @@ def tune(M, batch=1, candidates=None, reps=10, force=False):
     return Q8Tuning(*entry["tuning"]), entry
 
 
-def tune_stack(make_stack, candidates=CANDIDATES, reps=10):
-    """Best tuning for a Q8Stack built by make_stack(tuning); returns (tuning, {cand: us per launch})."""
+def stack_key(matrices, batch):
+    """Cache key of a stack: GPU, library build, batch and a hash of every job's shape, table mode, segment
+    length and size (the order of the jobs is part of it: it is the order of the work queue)."""
+    import hashlib
+    M0 = matrices[0]
+    props = torch.cuda.get_device_properties(M0.device)
+    cap = torch.cuda.get_device_capability(M0.device)
+    h = hashlib.sha1()
+    for M in matrices:
+        h.update(f"{M.rows}x{M.cols}|{M.local}|{M.seg_quads}|{M.max_blk_rows}|{M.payload_bytes};".encode())
+    return f"{props.name}|sm{cap[0]}{cap[1]}|{_build_id()}|stack{len(matrices)}:{h.hexdigest()[:16]}|B{batch}"
+
+
+def tune_stack(make_stack, candidates=CANDIDATES, reps=10, key=None, force=False):
+    """Best tuning for a Q8Stack built by make_stack(tuning); returns (tuning, {cand: us per launch}).  With a
+    key (stack_key), a cached result is reused and a new one stored in the same cache as single matrices."""
+    if key is not None and not force:
+        with _lock:
+            db = _load()
+        if key in db:
+            return tuple(db[key]["tuning"]), db[key]["all"]
     results = {}
     for cand in candidates:
         try:
@@ -164,4 +183,7 @@ def tune_stack(make_stack, candidates=CANDIDATES, reps=10):
             continue
         results[",".join(map(str, cand))] = 1e3 * ms
     best = min(results, key=results.get)
-    return tuple(int(v) for v in best.split(",")), results
+    tuning = tuple(int(v) for v in best.split(","))
+    if key is not None:
+        _update(key, {"tuning": list(tuning), "us": results[best], "all": results})
+    return tuning, results

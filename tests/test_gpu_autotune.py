@@ -49,3 +49,26 @@ def test_tune_stack_picks_a_launchable_candidate():
                                     candidates=autotune.candidates_for(8, autotune.CANDIDATES), reps=2)
     assert ",".join(map(str, best)) in res and len(res) >= 8
     assert ops.device_status() == 0
+
+
+def test_tune_stack_caches_by_stack_key(tmp_path, monkeypatch):
+    monkeypatch.setenv("MATVANS_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    rng = np.random.default_rng(14)
+    Ws = [np.clip(np.round(rng.normal(0, 3, size=sh)), -127, 127).astype(np.int8) for sh in ((256, 512), (96, 1024))]
+    Ms = [ops.Q8Matrix.encode(W) for W in Ws]
+    key = autotune.stack_key(Ms, 1)
+    assert key != autotune.stack_key(Ms, 4) and key != autotune.stack_key(Ms[::-1], 1)
+    built = []
+    make = lambda t: built.append(t) or ops.Q8Stack(Ms, batch=1, tuning=t)  # noqa: E731
+    cands = [(4, 1, 1, 0, 0, 0), (8, 2, 1, 0, 0, 0), (16, 1, 1, 0, 0, 0)]
+    best, res = autotune.tune_stack(make, candidates=cands, reps=2, key=key)
+    assert len(built) == 3 and best in cands
+    built.clear()
+    best2, res2 = autotune.tune_stack(make, candidates=cands, reps=2, key=key)
+    assert not built and best2 == best and res2 == res  # served from the cache
+    xs = [torch.from_numpy(rng.integers(-127, 128, size=(1, W.shape[1])).astype(np.int8)).cuda() for W in Ws]
+    S = ops.Q8Stack(Ms, batch=1, tuning=best2, xs=xs)
+    S.run()
+    for W, x, y in zip(Ws, xs, S.ys):
+        assert np.array_equal(y.cpu().numpy(), oracle.matvec_i8(W, x.cpu().numpy()))
+    assert ops.device_status() == 0
