@@ -914,6 +914,8 @@ def run_profile_kernel(args):
     import oracle
     dev = torch.device("cuda", 0)
     rng = np.random.default_rng(11)
+    if args.profile_kernel in ("float1", "chain", "stripes", "fallback"):
+        return run_profile_more(args, torch, ops, oracle, dev, rng)
     if args.profile_kernel == "float":
         shape = (11008, 4096)
         W = gen_matrix(shape, 4.0, 21)
@@ -957,6 +959,66 @@ def run_profile_kernel(args):
     return 0
 
 
+def run_profile_more(args, torch, ops, oracle, dev, rng):
+    """More small cases for ncu, each gated first:
+    float1    4096x11008 sigma 4, per-row tables, one bf16 vector: forward and re-decoding backward (CUDA cores)
+    chain     the 4096 -> 11008 -> 4096 chain (q, gate-shaped, down-shaped matrices) fused in one cooperative launch
+    stripes   the reference's ans-warp-stripes layout, 4096x4096 sigma 4, one vector
+    fallback  the non-persistent Q8 kernel (columns not a multiple of 16: 4096x4100), one vector"""
+    kind = args.profile_kernel
+    if kind == "float1":
+        shape = (4096, 11008)
+        W = gen_matrix(shape, 4.0, 23)
+        M = ops.Q8Matrix.encode(W, local=True, device=dev)
+        s = torch.from_numpy(rng.uniform(1e-3, 1e-2, shape[0]).astype(np.float32)).to(dev)
+        X = torch.from_numpy(rng.standard_normal((1, shape[1])).astype(np.float32)).to(torch.bfloat16).to(dev)
+        dY = torch.from_numpy(rng.standard_normal((1, shape[0])).astype(np.float32)).to(torch.bfloat16).to(dev)
+        Wd = torch.from_numpy(W).to(dev).double()
+        ref = (X.double() @ Wd.T) * s.double()[None, :]
+        if not torch.allclose(M.matvec_bf16(X, s).double(), ref, rtol=1e-4, atol=1e-4 * ref.abs().max().item()):
+            raise SystemExit("bench: float forward (B=1) disagrees with the FP64 product")
+        refb = (dY.double() * s.double()[None, :]) @ Wd
+        if not torch.allclose(M.matvec_t_bf16(dY, s).double(), refb, rtol=1e-4, atol=1e-4 * refb.abs().max().item()):
+            raise SystemExit("bench: float backward (B=1) disagrees with the FP64 product")
+        run = lambda: (M.matvec_bf16(X, s), M.matvec_t_bf16(dY, s))  # noqa: E731
+    elif kind == "chain":
+        shapes = [(4096, 4096), (11008, 4096), (4096, 11008)]
+        Ws = [gen_matrix(sh, 4.0, 30 + i) for i, sh in enumerate(shapes)]
+        Ms = [ops.Q8Matrix.encode(W, local=True, device=dev) for W in Ws]
+        x0 = torch.from_numpy(rng.integers(-127, 128, size=(1, 4096)).astype(np.int8)).to(dev)
+        C = ops.Q8Chain(Ms, [2e-3] * 3, batch=1, x0=x0, device=dev)
+        C.run()
+        torch.cuda.synchronize()
+        v = x0.cpu().numpy()
+        for W in Ws:
+            y = oracle.matvec_i8(W, v)
+            v = np.clip(np.rint(y.astype(np.float32) * np.float32(2e-3)), -128, 127).astype(np.int8)
+        if not np.array_equal(C.out8.cpu().numpy(), v):
+            raise SystemExit("bench: chain is not bit-exact")
+        run = C.run
+    elif kind == "stripes":
+        W = gen_matrix((4096, 4096), 4.0, 24)
+        A = ops.AwsMatrix.encode(W, device=dev)
+        x = rng.integers(-127, 128, size=(1, 4096)).astype(np.int8)
+        xd = torch.from_numpy(x).to(dev)
+        if not np.array_equal(A.matvec(xd).cpu().numpy(), oracle.matvec_i8(W, x)):
+            raise SystemExit("bench: stripes kernel is not bit-exact")
+        run = lambda: A.matvec(xd)  # noqa: E731
+    else:
+        W = gen_matrix((4096, 4100), 4.0, 25)
+        M = ops.Q8Matrix.encode(W, local=True, device=dev)
+        x = rng.integers(-127, 128, size=(1, 4100)).astype(np.int8)
+        xd = torch.from_numpy(x).to(dev)
+        if not np.array_equal(M.matvec(xd).cpu().numpy(), oracle.matvec_i8(W, x)):
+            raise SystemExit("bench: fallback kernel is not bit-exact")
+        run = lambda: M.matvec(xd)  # noqa: E731
+    for _ in range(2):
+        run()
+    torch.cuda.synchronize()
+    ops.device_status()
+    return 0
+
+
 def run_profile_stack(args):
     """Small fixed stack case for ncu: gate + two plain steps."""
     import torch
@@ -991,7 +1053,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stack", action="store_true",
                     help="skip the 224-matrix batched stack and the large low-entropy sections")
-    ap.add_argument("--profile-kernel", default="", choices=["", "awr", "wpr", "dense", "float"],
+    ap.add_argument("--profile-kernel", default="",
+                    choices=["", "awr", "wpr", "dense", "float", "float1", "chain", "stripes", "fallback"],
                     help="small fixed case of one kernel family (the case ncu captures)")
     ap.add_argument("--profile-stack", default="",
                     help="LAYERS,B,ENGINE[,WARPS]: build a stack of LAYERS x 7 matrices and run two steps at B "
