@@ -260,7 +260,12 @@ typedef struct mv_q8_stack_info {
 
 /* Plans a batched launch on the host: fills ngroups/atomic/item0 of every
  * job for the given tuning and returns the sizes the launch needs.  The
- * caller then copies `jobs` to device memory. */
+ * caller then copies `jobs` to device memory.  The plan reorders the array in
+ * place, jobs with the most work per item first (stable), so that the work
+ * queue ends on short items; every job keeps its own x and y, so results are
+ * unaffected.  It also zeroes jobs[0].pad, the work-queue counter of the
+ * launch (reset by the kernel after each launch; concurrent launches on one
+ * job table race). */
 mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning,
                            mv_q8_stack_info *info);
 

@@ -1893,6 +1893,12 @@ mv_status launch_q8f(const Q8SLaunch &L, int mode, int nv, const mv_q8_tuning &t
 
 int nv_round(int nb) { return nb <= 2 ? nb : nb <= 4 ? 4 : nb <= 8 ? 8 : 16; }
 
+}  // namespace
+
+mv_status stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning, mv_q8_stack_info *info);
+
+namespace {
+
 mv_q8_tuning resolve(const mv_q8_tuning *t) {
     mv_q8_tuning r{8, 2, 1, 0, 0, MV_ENGINE_AUTO};
     if (t) {
@@ -2049,6 +2055,25 @@ mv_status mv_q8_matvec_t_bf16(const mv_q8_view *m, const uint16_t *dy_dev, int b
 
 mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning, mv_q8_stack_info *info) {
     if (!jobs || njobs <= 0 || !info) return mv::fail(MV_ERR_ARG, "mv_q8_stack_plan: bad arguments");
+    // The work queue hands out items in job order: jobs with the most work per item (decode steps of a
+    // stripe's segment group) go first, so that the last items taken, which set the end of the launch, are
+    // the shortest (stable: equal jobs keep their order).  Each job carries its own x and y, so the outputs
+    // do not depend on the order.
+    std::stable_sort(jobs, jobs + njobs, [&](const mv_q8_job &a, const mv_q8_job &b) {
+        auto work = [&](const mv_q8_job &j) {
+            const int parts = std::max(1, std::min(tuning && tuning->parts > 0 ? tuning->parts : 1, std::max(1, j.m.nseg)));
+            return (long long)((std::max(1, j.m.nseg) + parts - 1) / parts) * std::max(1, j.m.seg_quads);
+        };
+        return work(a) > work(b);
+    });
+    return mv::stack_plan(jobs, njobs, tuning, info);
+}
+
+}  // extern "C"
+
+namespace mv {
+
+mv_status stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tuning, mv_q8_stack_info *info) {
     const mv_q8_tuning t = mv::resolve(tuning);
     uint32_t item = 0;
     info->max_blk_rows = 2;
@@ -2076,6 +2101,10 @@ mv_status mv_q8_stack_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
     return MV_OK;
 }
 
+}  // namespace mv
+
+extern "C" {
+
 size_t mv_q8_x_tiles_bytes(const mv_q8_view *m) {
     if (!m || m->nseg <= 0 || m->seg_quads <= 0) return 0;
     return (size_t)m->nseg * (size_t)((m->seg_quads + 31) / 32) * 2048;
@@ -2090,7 +2119,7 @@ mv_status mv_q8_chain_plan(mv_q8_job *jobs, int njobs, const mv_q8_tuning *tunin
     mv_q8_tuning t = mv::resolve(tuning);
     if (t.parts > 1) return mv::fail(MV_ERR_ARG, "mv_q8_chain_plan: a chain needs whole stripes (parts <= 1)");
     t.parts = 0;
-    return mv_q8_stack_plan(jobs, njobs, &t, info);
+    return mv::stack_plan(jobs, njobs, &t, info);  // a chain keeps its order
 }
 
 mv_status mv_q8_chain_matvec(mv_q8_job *jobs_dev, int njobs, const mv_q8_stack_info *info, int batch,

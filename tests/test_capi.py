@@ -49,9 +49,14 @@ def test_stack_plan_reports_atomic_jobs():
     assert L.mv_q8_stack_plan(jobs, 3, ctypes.byref(Q8Tuning(8, 1, 1, 0, 0, 0)), ctypes.byref(info)) == 0
     assert info.atomic_jobs == 0 and all(jobs[i].atomic == 0 for i in range(3))
     assert info.nitems == 2 + 1 + 3
+    # the plan orders the jobs by work per item, most first (whole stripes: by columns), and numbers the
+    # items job by job in that order
+    assert [jobs[i].m.cols for i in range(3)] == [1024, 512, 64]
+    assert [jobs[i].item0 for i in range(3)] == [0, 3, 5]
     # parts = 4: every job with more than one segment is split (and accumulates atomically); the
     # 64-column job has a single segment and stays whole
     assert L.mv_q8_stack_plan(jobs, 3, ctypes.byref(Q8Tuning(8, 1, 1, 0, 4, 0)), ctypes.byref(info)) == 0
-    assert [jobs[i].ngroups for i in range(3)] == [4, 1, 4]
-    assert info.atomic_jobs == 2 and [jobs[i].atomic for i in range(3)] == [1, 0, 1]
+    by_cols = {jobs[i].m.cols: jobs[i] for i in range(3)}
+    assert [by_cols[c].ngroups for c in (512, 64, 1024)] == [4, 1, 4]
+    assert info.atomic_jobs == 2 and [by_cols[c].atomic for c in (512, 64, 1024)] == [1, 0, 1]
     assert info.nitems == 2 * 4 + 1 + 3 * 4
