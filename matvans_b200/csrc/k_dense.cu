@@ -105,6 +105,7 @@ struct DevInfo {
     uint32_t *status = nullptr;
     int sms = 0;
     int smem_optin = 0;
+    int smem_sm = 0;
 };
 
 std::mutex g_mu;
@@ -122,6 +123,7 @@ DevInfo *dev_info(mv_status *st) {
     if (!di.sms) {
         cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, d);
         cudaDeviceGetAttribute(&di.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d);
+        cudaDeviceGetAttribute(&di.smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, d);
     }
     *st = MV_OK;
     return &di;
@@ -165,6 +167,12 @@ int max_smem_optin() {
     mv_status st;
     DevInfo *di = dev_info(&st);
     return di && di->smem_optin ? di->smem_optin : 227 * 1024;
+}
+
+int max_smem_per_sm() {
+    mv_status st;
+    DevInfo *di = dev_info(&st);
+    return di && di->smem_sm ? di->smem_sm : 228 * 1024;
 }
 
 mv_status prepare_kernel(const void *kern, size_t smem, int threads, int *blocks_per_sm) {

@@ -57,6 +57,7 @@ constexpr uint32_t kStageOffs = 40;  // u32 per staging area: 33 relative offset
 constexpr uint32_t kStagePad = 8;    // entries per staging area beyond tbl_stage (copies start at an even entry)
 struct Q8SLayout {
     uint32_t extra, bufs, red, bars, ring, curs, sched, stage_o, rows, stage_e, total;
+    uint32_t async_tables;  // 1: two staging areas, the next item's table data staged during the current item
 };
 
 __global__ void scale_rows_kernel(const int32_t *y, const float *s, float *ys, int rows, int batch, int ldy);
@@ -1320,7 +1321,7 @@ __global__ void q8s_chain_reset(Q8Job *jobs, int njobs) {
 // Shared-memory layout of q8s_kernel (byte offsets), computed on the host and passed with the launch.
 __host__ __device__ inline Q8SLayout q8s_layout(uint32_t lut_bytes, uint32_t extra_bytes, uint32_t tbl_alias, int W,
                                                 int DEPTH, int ILP, int buf_words, int red_nv, int red_bufs,
-                                                int tbl_stage) {
+                                                int tbl_stage, bool two_areas = true) {
     Q8SLayout o{};
     uint32_t p = lut_bytes;
     o.extra = p;
@@ -1344,14 +1345,16 @@ __host__ __device__ inline Q8SLayout q8s_layout(uint32_t lut_bytes, uint32_t ext
     o.rows = p;  // [W][DEPTH][ILP] word-rows of each slot's blocks
     p += (uint32_t)(W * DEPTH * ILP) * 4u;
     p = (p + 15u) & ~15u;
-    // table staging: two areas (one item ahead), or one inside the consumer's region when that is free at
-    // table rebuilds and large enough (staged synchronously then)
+    // table staging: two areas (staged one item ahead, asynchronously), or one inside the consumer's region
+    // when that is free at table rebuilds and large enough, or one area of its own (staged synchronously)
     const uint32_t stage_bytes = ((uint32_t)tbl_stage + kStagePad) * 2u;
+    o.async_tables = 0;
     if (tbl_alias >= stage_bytes) {
         o.stage_e = o.extra;
     } else {
         o.stage_e = p;
-        p += 2u * stage_bytes;
+        o.async_tables = two_areas ? 1u : 0u;
+        p += (two_areas ? 2u : 1u) * stage_bytes;
     }
     o.total = p;
     return o;
@@ -1527,7 +1530,7 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
     // decode table at the start of shared memory: 256 quantiles x 32 lanes of 4 B (narrow) or 8 B (wide); the
     // rest of the layout comes with the launch (L.lay), so its offsets are constant-bank operands.
     // Two staging areas: the next item's table data is staged while the current item decodes.
-    const bool async_tbl = L.lay.stage_e != L.lay.extra;
+    const bool async_tbl = L.lay.async_tables != 0;
     uint32_t *lut = reinterpret_cast<uint32_t *>(smem);
     unsigned char *extra = smem + L.lay.extra;
     ItemRec *ring = reinterpret_cast<ItemRec *>(smem + L.lay.ring);
@@ -1793,9 +1796,19 @@ mv_status launch_q8s_t(const Q8SLaunch &L0, int W, int ctas_per_sm, cudaStream_t
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch: consumer region of %zu B breaks 16-byte alignment",
                     Cons::extra_bytes(W));
     Q8SLaunch L = L0;
-    L.lay = q8s_layout(Cons::kWideLut ? 256 * 32 * 8 : 256 * 32 * 4, (uint32_t)Cons::extra_bytes(W),
-                       (uint32_t)Cons::tbl_alias_bytes(W), W, DEPTH, ILP, L.buf_words, Cons::kRedNV, Cons::kRedBufs,
-                       L.tbl_stage);
+    auto layout = [&](bool two) {
+        return q8s_layout(Cons::kWideLut ? 256 * 32 * 8 : 256 * 32 * 4, (uint32_t)Cons::extra_bytes(W),
+                          (uint32_t)Cons::tbl_alias_bytes(W), W, DEPTH, ILP, L.buf_words, Cons::kRedNV,
+                          Cons::kRedBufs, L.tbl_stage, two);
+    };
+    L.lay = layout(true);
+    {
+        // asynchronous table staging needs a second area: keep it only if it costs no resident CTA
+        const Q8SLayout one = layout(false);
+        const int per_sm = max_smem_per_sm(), reserved = 1024;
+        if (L.lay.async_tables && per_sm / (int)(L.lay.total + reserved) < per_sm / (int)(one.total + reserved))
+            L.lay = one;
+    }
     L.slot_bytes = (uint32_t)ILP * (uint32_t)L.buf_words * 4u;
     L.stage_len = (uint32_t)L.tbl_stage + kStagePad;
     const size_t smem = L.lay.total;

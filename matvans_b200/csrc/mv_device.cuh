@@ -89,6 +89,7 @@ uint32_t wait_spin_limit();   // kWaitSpinLimit unless MV_INJECT_WAIT_LIMIT set 
 int inject_drop_copy();
 int sm_count();
 int max_smem_optin();
+int max_smem_per_sm();
 // Raise the kernel's dynamic shared-memory limit to `smem` (once per kernel
 // and device) and, if blocks_per_sm is non-NULL, return its occupancy for
 // `threads` threads (cached).  Safe to call while a stream is being captured.
