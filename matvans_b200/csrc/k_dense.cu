@@ -6,7 +6,8 @@
 // baselines/baseline_int8/baseline_matVec_custom.cu:99-155, written for
 // sm_100a: 16-byte streaming loads that bypass L1 (ld.global.nc.L1::no_allocate),
 // four loads in flight per lane, x staged in shared memory, any number of
-// vectors per pass sharing one read of W.
+// vectors per pass sharing one read of W; from four vectors on, each warp
+// takes four rows at once so that an x chunk read serves four W chunks.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -83,6 +84,62 @@ __global__ void __launch_bounds__(256) dense_kernel(const int8_t *__restrict__ W
     }
 }
 
+// Several vectors: a warp takes R rows at once, so that every x chunk it reads (shared memory, or the
+// caches) serves R rows; each lane holds R x NV accumulators and reads R W chunks per step (R streaming
+// loads in flight).  With one row per warp, 16 vectors cost 16 x-chunk reads per W chunk and the kernel was
+// bound by shared memory, not by HBM.
+template <int NV, int R, bool XG>
+__global__ void __launch_bounds__(256) dense_kernel_rows(const int8_t *__restrict__ W, int rows, int cols,
+                                                         const int8_t *__restrict__ x, int batch,
+                                                         int32_t *__restrict__ y) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint4 *xs = reinterpret_cast<uint4 *>(smem);  // [NV][cols/16] unless XG
+    const uint4 *xg = reinterpret_cast<const uint4 *>(x);
+    const int chunks = cols >> 4;
+    if (!XG) {
+        for (int i = threadIdx.x; i < NV * chunks; i += blockDim.x) {
+            const int v = i / chunks;
+            xs[i] = v < batch ? xg[i] : make_uint4(0, 0, 0, 0);
+        }
+        __syncthreads();
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int r0 = (blockIdx.x * nw + warp) * R; r0 < rows; r0 += gridDim.x * nw * R) {
+        int acc[R][NV];
+#pragma unroll
+        for (int r = 0; r < R; r++)
+#pragma unroll
+            for (int v = 0; v < NV; v++) acc[r][v] = 0;
+        const uint4 *wr[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) wr[r] = reinterpret_cast<const uint4 *>(W + (size_t)min(r0 + r, rows - 1) * cols);
+        for (int i = lane; i < chunks; i += 32) {
+            uint4 a[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) a[r] = ldg_nc_u4(wr[r] + i);  // rows past the end reread the last row
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const uint4 b = x_chunk<NV, XG>(xs, xg, v, chunks, i, batch);
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    acc[r][v] = __dp4a((int)a[r].x, (int)b.x, acc[r][v]);
+                    acc[r][v] = __dp4a((int)a[r].y, (int)b.y, acc[r][v]);
+                    acc[r][v] = __dp4a((int)a[r].z, (int)b.z, acc[r][v]);
+                    acc[r][v] = __dp4a((int)a[r].w, (int)b.w, acc[r][v]);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++)
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[r][v] += __shfl_xor_sync(0xffffffffu, acc[r][v], o);
+                if (lane == 0 && v < batch && r0 + r < rows) y[(size_t)v * rows + r0 + r] = acc[r][v];
+            }
+    }
+}
+
 namespace {
 
 template <int NV>
@@ -91,6 +148,18 @@ mv_status launch_dense(const int8_t *W, int rows, int cols, const int8_t *x, int
     const int nw = 8;
     const bool xg = (size_t)NV * cols > (size_t)max_smem_optin();
     const size_t smem = xg ? 0 : (size_t)NV * cols;
+    if constexpr (NV >= 4) {
+        constexpr int R = 4;
+        auto kern = xg ? dense_kernel_rows<NV, R, true> : dense_kernel_rows<NV, R, false>;
+        int bps = 0;
+        mv_status rc = prepare_kernel((const void *)kern, smem, 32 * nw, &bps);
+        if (rc) return rc;
+        const int groups = (rows + R - 1) / R;
+        const int grid = std::max(1, std::min((groups + nw - 1) / nw, std::max(1, bps) * sm_count()));
+        kern<<<grid, 32 * nw, smem, st>>>(W, rows, cols, x, batch, y);
+        MV_CUDA_TRY(cudaGetLastError(), "dense kernel launch");
+        return MV_OK;
+    }
     auto kern = xg ? dense_kernel<NV, true> : dense_kernel<NV, false>;
     int bps = 0;
     mv_status rc = prepare_kernel((const void *)kern, smem, 32 * nw, &bps);
