@@ -6,8 +6,8 @@
 // baselines/baseline_int8/baseline_matVec_custom.cu:99-155, written for
 // sm_100a: 16-byte streaming loads that bypass L1 (ld.global.nc.L1::no_allocate),
 // four loads in flight per lane, x staged in shared memory, any number of
-// vectors per pass sharing one read of W; from four vectors on, each warp
-// takes four rows at once so that an x chunk read serves four W chunks.
+// vectors per pass sharing one read of W; from eight vectors on, each lane
+// takes four rows of a column chunk, so that an x chunk read serves four rows.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -84,58 +84,112 @@ __global__ void __launch_bounds__(256) dense_kernel(const int8_t *__restrict__ W
     }
 }
 
-// Several vectors: a warp takes R rows at once, so that every x chunk it reads (shared memory, or the
-// caches) serves R rows; each lane holds R x NV accumulators and reads R W chunks per step (R streaming
-// loads in flight).  With one row per warp, 16 vectors cost 16 x-chunk reads per W chunk and the kernel was
-// bound by shared memory, not by HBM.
-template <int NV, int R, bool XG>
-__global__ void __launch_bounds__(256) dense_kernel_rows(const int8_t *__restrict__ W, int rows, int cols,
-                                                         const int8_t *__restrict__ x, int batch,
-                                                         int32_t *__restrict__ y) {
+// Reduce-scatter step over lane bit `o`: with N >= 2 sums held, each lane keeps the half of them its bit
+// selects and adds its partner's copy of that half (N/2 shuffles); with one, a plain butterfly.
+template <int N, int M>
+__device__ __forceinline__ void scatter_step(int (&acc)[M], int o, bool bit) {
+    if constexpr (N >= 2) {
+#pragma unroll
+        for (int j = 0; j < N / 2; j++) {
+            const int send = bit ? acc[j] : acc[j + N / 2];
+            const int keep = bit ? acc[j + N / 2] : acc[j];
+            acc[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    } else {
+        acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], o);
+    }
+}
+
+// Eight or more vectors: each lane takes R = 4 rows of the same 16-byte column chunk, so that an x chunk read
+// from shared memory (16 bytes per vector) serves four W chunks in registers: 16 vectors cost one
+// shared-memory wavefront per 4 dp4a instead of one per dp4a, and the kernel becomes bound by the dp4a
+// rate (64 per SM and clock: 4.6 TB/s of W at 16 vectors), not by shared memory.  Lane l reads chunks
+// l, l + 32, ... of its warp's four rows (each load instruction covers 512 contiguous bytes of one row);
+// the next chunks' loads are issued before the current ones are used.  x sits in shared memory in
+// slices of `slice` chunks (all of x when it fits, staged once; otherwise the CTA's 32 rows walk the
+// slices, restaged per slice).  The warp's 4 x NV row sums meet in one reduce-scatter over the five lane
+// bits: 62 shuffles at 16 vectors (instead of 320 for separate butterflies), two sums per lane.
+template <int NV>
+__global__ void __launch_bounds__(256, 2) dense_kernel_rows(const int8_t *__restrict__ W, int rows, int cols,
+                                                            const int8_t *__restrict__ x, int batch,
+                                                            int32_t *__restrict__ y, int slice) {
+    constexpr int R = 4, M = R * NV;
     extern __shared__ __align__(16) unsigned char smem[];
-    uint4 *xs = reinterpret_cast<uint4 *>(smem);  // [NV][cols/16] unless XG
+    uint4 *xs = reinterpret_cast<uint4 *>(smem);  // [NV][slice]
     const uint4 *xg = reinterpret_cast<const uint4 *>(x);
     const int chunks = cols >> 4;
-    if (!XG) {
-        for (int i = threadIdx.x; i < NV * chunks; i += blockDim.x) {
-            const int v = i / chunks;
-            xs[i] = v < batch ? xg[i] : make_uint4(0, 0, 0, 0);
-        }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    // scatter steps while two or more sums are held (up to the five lane bits); sum k = r * NV + v
+    constexpr int kSteps = M >= 32 ? 5 : M >= 16 ? 4 : M >= 8 ? 3 : 2;
+    constexpr int kHeld = M >> kSteps;
+    const int base = (lane >> (5 - kSteps)) * kHeld;
+    const bool writer = (lane & ((1 << (5 - kSteps)) - 1)) == 0;
+    const bool one_slice = chunks <= slice;
+    auto stage = [&](int c0, int n) {
+        for (int v = 0; v < NV; v++)
+            for (int i = threadIdx.x; i < n; i += blockDim.x)
+                xs[v * slice + i] = v < batch ? xg[(size_t)v * chunks + c0 + i] : make_uint4(0, 0, 0, 0);
+    };
+    if (one_slice) {
+        stage(0, chunks);
         __syncthreads();
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int r0 = (blockIdx.x * nw + warp) * R; r0 < rows; r0 += gridDim.x * nw * R) {
-        int acc[R][NV];
+    const int items = (rows + R * nw - 1) / (R * nw);  // 32 rows per CTA item: every warp loops alike
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+        const int r0 = (item * nw + warp) * R;
+        // chunk offsets of the four rows from the first (rows past the end reread the last row, store nothing)
+        const int rb = min(r0, rows - 1);
+        const uint4 *w0 = reinterpret_cast<const uint4 *>(W + (size_t)rb * cols);
+        int off[R];
 #pragma unroll
-        for (int r = 0; r < R; r++)
+        for (int r = 0; r < R; r++) off[r] = (min(r0 + r, rows - 1) - rb) * chunks;
+        int acc[M];
 #pragma unroll
-            for (int v = 0; v < NV; v++) acc[r][v] = 0;
-        const uint4 *wr[R];
+        for (int k = 0; k < M; k++) acc[k] = 0;
+        for (int c0 = 0; c0 < chunks; c0 += slice) {
+            const int n = min(slice, chunks - c0);
+            if (!one_slice) {
+                __syncthreads();  // the previous slice is consumed
+                stage(c0, n);
+                __syncthreads();
+            }
+            uint4 a[R], nx[R];
+            int i = lane;
+            if (i < n) {
 #pragma unroll
-        for (int r = 0; r < R; r++) wr[r] = reinterpret_cast<const uint4 *>(W + (size_t)min(r0 + r, rows - 1) * cols);
-        for (int i = lane; i < chunks; i += 32) {
-            uint4 a[R];
+                for (int r = 0; r < R; r++) a[r] = ldg_nc_u4(w0 + off[r] + c0 + i);
+            }
+            for (; i < n; i += 32) {
+                if (i + 32 < n) {
 #pragma unroll
-            for (int r = 0; r < R; r++) a[r] = ldg_nc_u4(wr[r] + i);  // rows past the end reread the last row
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                const uint4 b = x_chunk<NV, XG>(xs, xg, v, chunks, i, batch);
-#pragma unroll
-                for (int r = 0; r < R; r++) {
-                    acc[r][v] = __dp4a((int)a[r].x, (int)b.x, acc[r][v]);
-                    acc[r][v] = __dp4a((int)a[r].y, (int)b.y, acc[r][v]);
-                    acc[r][v] = __dp4a((int)a[r].z, (int)b.z, acc[r][v]);
-                    acc[r][v] = __dp4a((int)a[r].w, (int)b.w, acc[r][v]);
+                    for (int r = 0; r < R; r++) nx[r] = ldg_nc_u4(w0 + off[r] + c0 + i + 32);
                 }
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const uint4 b = xs[v * slice + i];
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
+                        int &c = acc[r * NV + v];
+                        c = __dp4a((int)a[r].x, (int)b.x, c);
+                        c = __dp4a((int)a[r].y, (int)b.y, c);
+                        c = __dp4a((int)a[r].z, (int)b.z, c);
+                        c = __dp4a((int)a[r].w, (int)b.w, c);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; r++) a[r] = nx[r];
             }
         }
+        scatter_step<M, M>(acc, 16, (lane & 16) != 0);
+        scatter_step<(M >= 2 ? M / 2 : 1), M>(acc, 8, (lane & 8) != 0);
+        scatter_step<(M >= 4 ? M / 4 : 1), M>(acc, 4, (lane & 4) != 0);
+        scatter_step<(M >= 8 ? M / 8 : 1), M>(acc, 2, (lane & 2) != 0);
+        scatter_step<(M >= 16 ? M / 16 : 1), M>(acc, 1, (lane & 1) != 0);
+        if (writer)
 #pragma unroll
-        for (int r = 0; r < R; r++)
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc[r][v] += __shfl_xor_sync(0xffffffffu, acc[r][v], o);
-                if (lane == 0 && v < batch && r0 + r < rows) y[(size_t)v * rows + r0 + r] = acc[r][v];
+            for (int j = 0; j < kHeld; j++) {
+                const int k = base + j, r = k / NV, v = k % NV;
+                if (v < batch && r0 + r < rows) y[(size_t)v * rows + r0 + r] = acc[j];
             }
     }
 }
@@ -146,20 +200,23 @@ template <int NV>
 mv_status launch_dense(const int8_t *W, int rows, int cols, const int8_t *x, int batch, int32_t *y,
                        cudaStream_t st) {
     const int nw = 8;
-    const bool xg = (size_t)NV * cols > (size_t)max_smem_optin();
-    const size_t smem = xg ? 0 : (size_t)NV * cols;
-    if constexpr (NV >= 4) {
-        constexpr int R = 4;
-        auto kern = xg ? dense_kernel_rows<NV, R, true> : dense_kernel_rows<NV, R, false>;
+    if constexpr (NV >= 8) {
+        // x slices of at most 64 KB (NV x slice x 16 bytes): two CTAs per SM.  (At 4 vectors the warp-per-row
+        // kernel below measured faster: 0.55 vs 0.71 ms over 56 matrices of the 7B stack.)
+        const int chunks = cols / 16, slice = std::min(chunks, 4096 / NV);
+        const size_t smem = (size_t)NV * slice * 16;
+        auto kern = dense_kernel_rows<NV>;
         int bps = 0;
         mv_status rc = prepare_kernel((const void *)kern, smem, 32 * nw, &bps);
         if (rc) return rc;
-        const int groups = (rows + R - 1) / R;
-        const int grid = std::max(1, std::min((groups + nw - 1) / nw, std::max(1, bps) * sm_count()));
-        kern<<<grid, 32 * nw, smem, st>>>(W, rows, cols, x, batch, y);
+        const int items = (rows + 4 * nw - 1) / (4 * nw);  // four rows per warp
+        const int grid = std::max(1, std::min(items, std::max(1, bps) * sm_count()));
+        kern<<<grid, 32 * nw, smem, st>>>(W, rows, cols, x, batch, y, slice);
         MV_CUDA_TRY(cudaGetLastError(), "dense kernel launch");
         return MV_OK;
     }
+    const bool xg = (size_t)NV * cols > (size_t)max_smem_optin();
+    const size_t smem = xg ? 0 : (size_t)NV * cols;
     auto kern = xg ? dense_kernel<NV, true> : dense_kernel<NV, false>;
     int bps = 0;
     mv_status rc = prepare_kernel((const void *)kern, smem, 32 * nw, &bps);
@@ -277,10 +334,8 @@ mv_status dense_matvec(const int8_t *W, int rows, int cols, const int8_t *x, int
     if (cols % 16) return fail(MV_ERR_SHAPE, "mv_dense_matvec: cols %% 16 != 0");
     if (((uintptr_t)W & 15) || ((uintptr_t)x & 15))
         return fail(MV_ERR_ARG, "mv_dense_matvec: W and x must be 16-byte aligned");
-    // vectors per pass: up to 16, fewer when their x does not fit shared memory (x is then read through the
-    // caches only if a single vector does not fit)
-    int pass = 16;
-    while (pass > 1 && (size_t)pass * cols > (size_t)max_smem_optin()) pass >>= 1;
+    // up to 16 vectors per pass share one read of W (x that does not fit shared memory is read through L1)
+    const int pass = 16;
     for (int v0 = 0; v0 < batch; v0 += pass) {
         const int nb = std::min(pass, batch - v0);
         const int8_t *xv = x + (size_t)v0 * cols;
