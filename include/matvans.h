@@ -200,8 +200,9 @@ mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int3
                        const float *row_scales_dev, float *y_scaled_dev, void *stream);
 
 /* Launch parameters of the persistent Q8 kernel (0 = library default).
- *   warps        warps per CTA (1..8, default 8; up to 16 when the tensor-core
- *                engine runs, i.e. 8..16 vectors with engine 0)
+ *   warps        warps per CTA (default 8): up to 16 for the integer
+ *                CUDA-core consumer, up to 8 for the tensor-core engine and
+ *                the float form
  *   ilp          independent segments decoded per warp (1 or 2, default 2;
  *                1 for the float form)
  *   depth        shared-memory stream buffers per warp (1 or 2, default 1):

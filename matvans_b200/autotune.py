@@ -35,7 +35,7 @@ def candidates_for(batch, base):
     (engine 0, where ilp is fixed at 1) or on the CUDA cores (engine 1)."""
     if batch < 8:
         return list(base)
-    mma = sorted({(w, 1, c[2], c[3], c[4], 0) for c in base for w in (4, 6, 8, 16)})
+    mma = sorted({(w, 1, c[2], c[3], c[4], 0) for c in base for w in (4, 6, 8)})  # at most 8 warps
     return mma + [c[:5] + (1,) for c in base]
 L2_BYTES = 126 * 2 ** 20
 _lock = threading.Lock()

@@ -325,14 +325,41 @@ __device__ __forceinline__ uint32_t q8_step_wide(uint32_t &lo, uint32_t &hi, uin
     return __byte_perm(__byte_perm(e0.x, e1.x, 0x0062), __byte_perm(e2.x, e3.x, 0x0062), 0x5410);
 }
 
+// The narrow step over 4-byte entries at a 256-byte pitch: entry (q, lane) at byte q*256 + lane*4 from the
+// start of shared memory, so that one byte permute forms each address as in the wide layout (the other 128
+// bytes of each 256-byte row belong to the consumer).
+__device__ __forceinline__ uint32_t q8_step_n256(uint32_t &lo, uint32_t &hi, uint32_t &koff, const uint32_t kend,
+                                                 const unsigned char *lut_b, uint32_t lane4, uint32_t &P) {
+    q8_refill(lo, hi, koff, kend, lut_b);
+    const uint32_t e0 = *reinterpret_cast<const uint32_t *>(lut_b + __byte_perm(lo, lane4, 0x5504));
+    const uint32_t e1 = *reinterpret_cast<const uint32_t *>(lut_b + __byte_perm(lo, lane4, 0x5514));
+    const uint32_t e2 = *reinterpret_cast<const uint32_t *>(lut_b + __byte_perm(lo, lane4, 0x5524));
+    const uint32_t e3 = *reinterpret_cast<const uint32_t *>(lut_b + __byte_perm(lo, lane4, 0x5534));
+    // entry = f | sym << 16 | r << 24 (byte 1 zero, so the low half-word is exactly f)
+    const uint32_t r0 = __umulhi(e0, 256u), r1 = __umulhi(e1, 256u);
+    const uint32_t r2 = e2 >> 24, r3 = e3 >> 24;
+    const uint32_t u01 = __dp2a_lo(r1, e0, r0);     // r0 + f0*r1
+    const uint32_t t2 = __dp2a_lo(r3, e2, r2);      // r2 + f2*r3
+    const uint32_t p01 = __dp2a_lo(e1, e0, 0u);     // f1*f0
+    const uint32_t p23 = __dp2a_lo(e3, e2, 0u);     // f3*f2
+    P = p01 * p23;
+    const uint32_t t0 = u01 + p01 * t2;             // r0 + f0 r1 + f0 f1 (r2 + f2 r3) < P
+    const unsigned long long st = (unsigned long long)hi * P + t0;
+    lo = (uint32_t)st;
+    hi = (uint32_t)(st >> 32);
+    return __byte_perm(__byte_perm(e0, e1, 0x0062), __byte_perm(e2, e3, 0x0062), 0x5410);
+}
+
 // One step through whichever table layout the consumer uses; sm is the start of shared memory (where the
-// wide table sits), lut the lane's column of the narrow table.
-template <bool kWide>
+// wide and the 256-byte-pitch narrow tables sit), lut the lane's column of the 128-byte-pitch narrow table.
+template <bool kWide, bool k256 = false>
 __device__ __forceinline__ uint32_t q8_step_t(uint32_t &lo, uint32_t &hi, uint32_t &koff, const uint32_t kend,
                                               const unsigned char *sm, const uint32_t *lut, uint32_t stride, int lane,
                                               uint32_t &P) {
     if constexpr (kWide)
         return q8_step_wide(lo, hi, koff, kend, sm, (uint32_t)lane << 3, P);
+    else if constexpr (k256)
+        return q8_step_n256(lo, hi, koff, kend, sm, (uint32_t)lane << 2, P);
     else
         return q8_step(lo, hi, koff, kend, sm, lut, stride, P);
 }
@@ -370,6 +397,7 @@ struct IntCons {
     static constexpr int kMaxThreads = 512;  // up to 16 warps per CTA
     static constexpr int kTmemCols = 0;
     static constexpr bool kWideLut = true;
+    static constexpr bool kLut256 = false;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
@@ -454,6 +482,7 @@ struct FwdCons {
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
     static constexpr bool kWideLut = true;
+    static constexpr bool kLut256 = false;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
@@ -543,6 +572,7 @@ struct BwdCons {
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 0;
     static constexpr bool kWideLut = false;  // its shuffle reduction already loads the shared-memory pipe
+    static constexpr bool kLut256 = false;
     static __host__ __device__ constexpr size_t extra_bytes(int) { return 0; }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *, uint32_t, int, int, int) {}
@@ -687,59 +717,66 @@ __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const 
 // lane issues two tcgen05.mma.kind::i8 (K = 32 each) with A = that tile in
 // TMEM (M = 128: the warp's lane quarter holds its 32 rows, the other lanes
 // are never written and their results never read), B = the x tile in shared
-// memory (N = 16 vectors, K-major core matrices of 8 rows x 16 bytes, LBO
-// 128 B, SBO 256 B), accumulating exactly in int32 in the warp's own 16 TMEM
-// columns.  Each warp owns 32 TMEM columns: D [0,16) and the A tile [16,32).
-// One tcgen05.commit per 16 quads arrives on the warp's mbarrier; the A tile
-// is rewritten only after the previous pair of MMAs completed (issued a whole
-// 16-quad decode earlier, so the wait is normally already over).  x moves
-// through a 128-column window (4 x 32 columns x 16 vectors, 2 KB per warp);
-// the next window is loaded into registers while the current one is in use.
-// The x tiles double as the cross-warp reduction area and as the staging area
-// of the decode tables.  ILP 1 only.
+// memory (N = 16 vectors, K-major core matrices of 8 rows x 16 bytes),
+// accumulating exactly in int32 in the warp's own 16 TMEM columns.  Each warp
+// owns 32 TMEM columns: D [0,16) and the A tile [16,32).  One tcgen05.commit
+// per 16 quads arrives on the warp's mbarrier; the A tile is rewritten only
+// after the previous pair of MMAs completed (issued a whole 16-quad decode
+// earlier, so the wait is normally already over).  x moves through a
+// 128-column window (4 x 32 columns x 16 vectors, 2 KB per warp); the next
+// window is loaded while the current one is in use.  ILP 1 only.
+//
+// Shared memory: the decode table takes 4-byte entries at a 256-byte pitch
+// (entry (q, lane) at byte q*256 + lane*4, one byte permute per address), and
+// the x tiles live in the other half of each 256-byte row: 256 holes of 128
+// bytes, one core matrix each, 32 per warp (two tiles of 16), hence at most 8
+// warps.  A core matrix (n, k) of piece p of tile t of warp w sits in hole
+// w*32 + t*16 + p*4 + n*2 + k: LBO (K) 256 B, SBO (N) 512 B.  64 KB hold
+// table and x tiles, as much as the 32 KB table with separate x tiles, so two
+// 8-warp CTAs still fit an SM.  The holes also take the cross-warp reduction.
 struct MmaCons {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;      // reduction area: the x tiles
     static constexpr int kRedBufs = 1;
     static constexpr bool kFinishSyncs = true;
-    static constexpr int kMinCtas = 1;    // with up to 16 warps: at most 128 registers per thread
-    static constexpr int kMaxThreads = 512;  // 1 x 16 or 2 x 8 warps per SM
+    static constexpr int kMinCtas = 2;    // at most 128 registers per thread
+    static constexpr int kMaxThreads = 256;  // 32 holes per warp
     static constexpr int kTmemCols = 1;   // > 0: the kernel allocates TMEM
-    static constexpr bool kWideLut = false;  // two CTAs per SM: the 32 KB table
+    static constexpr bool kWideLut = false;
+    static constexpr bool kLut256 = true;  // 4-byte entries at a 256-byte pitch, x tiles in between
     static constexpr int kXChunks = 4;    // x tile: 4 pieces of 32 columns x 16 vectors (512 B each)
     static constexpr int kXBytes = kXChunks * 512;
+    static constexpr uint32_t kHoles = kXBytes / 128;  // core matrices per tile
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
-        // two x tiles of 2 KB per warp, three mbarriers per warp (MMA commits, x copies into tile 0 / 1),
-        // TMEM address slot (the last 128 bytes); a multiple of 128 bytes, so the stream buffers that
-        // follow stay 16-byte aligned for the bulk copies
-        return (((size_t)W * 2 * kXBytes + (size_t)W * 24 + 128) + 127) / 128 * 128;
+        // three mbarriers per warp (MMA commits, x copies into tile 0 / 1), TMEM address slot (the last 128
+        // bytes); a multiple of 128 bytes, so the stream buffers that follow stay 16-byte aligned
+        return (((size_t)W * 24 + 128) + 127) / 128 * 128;
     }
-    // the decode tables are staged in the x tiles when they fit
-    static __host__ __device__ constexpr size_t tbl_alias_bytes(int W) { return (size_t)W * 2 * kXBytes; }
+    static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     static __host__ __device__ constexpr uint32_t tmem_cols(int W) {
         return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : W <= 8 ? 256 : 512;
     }
+    // hole h: byte h*256 + 128 from the start of shared memory
+    static __device__ __forceinline__ uint32_t hole(uint32_t h) { return h * 256u + 128u; }
     uint32_t xt, d_tmem, st_addr, ld_addr, ncommit, xcur, xcnt0, xcnt1;
     uint64_t b_desc0;
     uint64_t *mbar, *xbar;
-    int *xbase;
-    unsigned char *xt_ptr;
+    unsigned char *sm0;  // start of shared memory (table and holes)
     const int8_t *x;
     const int8_t *tiles;  // x laid out per (segment, window) by q8s_build_x_tiles, or null
-    int cols, batch, job_idx, nwin;
+    int cols, batch, job_idx, nwin, hole0;
     bool any;
 
-    __device__ __forceinline__ void init(const Q8SLaunch &, unsigned char *extra, uint32_t tmem_base, int,
+    __device__ __forceinline__ void init(const Q8SLaunch &L, unsigned char *extra, uint32_t tmem_base, int,
                                          int lane, int W) {
         // the warp index through a shuffle from lane 0 is known warp-uniform to the compiler, so the MMA
         // operands derived from it stay in uniform registers
         const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
-        const uint32_t base = smem_u32(extra);
-        xbase = reinterpret_cast<int *>(extra);
-        xt = base + (uint32_t)warp * (uint32_t)(2 * kXBytes);
-        xt_ptr = extra + (size_t)warp * 2 * kXBytes;
-        mbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 2 * kXBytes) + warp;
-        xbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 2 * kXBytes + (size_t)W * 8) + 2 * warp;
+        sm0 = extra - L.lay.extra;  // the table (and its holes) starts shared memory
+        hole0 = warp * (int)(2 * kHoles);
+        xt = smem_u32(sm0) + hole((uint32_t)hole0);  // tile 0, core matrix 0
+        mbar = reinterpret_cast<uint64_t *>(extra) + warp;
+        xbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 8) + 2 * warp;
         if (lane == 0) {
             mbar_init(mbar, 1);
             mbar_init(&xbar[0], 1);
@@ -753,7 +790,7 @@ struct MmaCons {
         d_tmem = tmem_base + 32u * (uint32_t)warp;
         st_addr = d_tmem + 16u + quarter;
         ld_addr = d_tmem + quarter;
-        b_desc0 = umma_smem_desc(xt, 128u, 256u);
+        b_desc0 = umma_smem_desc(xt, 256u, 512u);
         ncommit = 0;
         xcur = 1;  // the x tile of the latest window; a segment's first window goes to the other one
         xcnt0 = xcnt1 = 0;
@@ -767,15 +804,16 @@ struct MmaCons {
         tiles = J.x_tiles;
         nwin = (J.m.seg_quads + 31) / 32;
     }
-    // Bulk copy (async proxy, one lane) of x window w of segment seg into tile t; every lane counts it.
-    // The tile's previous readers (MMAs) are done, and generic writes to it (reduction area, table
-    // staging) were fenced by every writer before the CTA barrier that ended them.
+    // Bulk copies (async proxy) of x window w of segment seg into tile t: lane c < 16 copies core matrix c
+    // (128 bytes) into its hole; lane 0 announces the 2 KB first.  Every lane counts the window.  The
+    // tile's previous readers (MMAs) are done, and generic writes to it (reduction area) were fenced by
+    // every writer before the CTA barrier that ended them.
     __device__ __forceinline__ void x_copy(int t, int seg, int w, int lane) {
-        if (lane == 0) {
-            mbar_arrive_expect_tx(&xbar[t], (uint32_t)kXBytes);
-            bulk_g2s(xt_ptr + (size_t)t * kXBytes, tiles + ((size_t)seg * nwin + w) * kXBytes, (uint32_t)kXBytes,
-                     &xbar[t]);
-        }
+        if (lane == 0) mbar_arrive_expect_tx(&xbar[t], (uint32_t)kXBytes);
+        __syncwarp();
+        if (lane < (int)kHoles)
+            bulk_g2s(sm0 + hole((uint32_t)(hole0 + t * (int)kHoles + lane)),
+                     tiles + ((size_t)seg * nwin + w) * kXBytes + (size_t)lane * 128, 128u, &xbar[t]);
         if (t) xcnt1++;
         else xcnt0++;
     }
@@ -795,11 +833,12 @@ struct MmaCons {
         __syncwarp();
         if (elect_one()) {
             tcgen05_fence_after();
-            // B descriptor start addresses are in 16-byte units: tile xcur is 2 KB in, piece p 512 B
+            // B descriptor start addresses are in 16-byte units: tile xcur is 16 holes (4 KB) in, piece p 4
+            // holes (1 KB)
             const uint32_t idesc = umma_idesc_i8(128, 16);
-            const uint64_t bd = b_desc0 + (uint64_t)(xcur * (kXBytes / 16) + piece * 32);
+            const uint64_t bd = b_desc0 + (uint64_t)(xcur * (kHoles * 16) + piece * 64);
             umma_i8_ts(d_tmem, d_tmem + 16u, bd, idesc, any ? 1u : 0u);
-            if (two) umma_i8_ts(d_tmem, d_tmem + 24u, bd + 32u, idesc, 1u);
+            if (two) umma_i8_ts(d_tmem, d_tmem + 24u, bd + 64u, idesc, 1u);  // the next piece, 1 KB on
             umma_commit(mbar);
         }
         __syncwarp();
@@ -836,7 +875,8 @@ struct MmaCons {
         const bool xok = b < batch;
         const int colbase = 4 * q0 + 16 * h;
         const int8_t *xrow = x + (size_t)(xok ? b : 0) * cols + colbase;
-        const uint32_t xdst = xt + (uint32_t)(b >> 3) * 256u + (uint32_t)h * 128u + (uint32_t)(b & 7) * 16u;
+        // core matrix (n, k) = (b / 8, h) of piece i in hole 4 i + 2 n + k of tile 0, row b % 8
+        const uint32_t xdst = xt + ((uint32_t)(b >> 3) * 2u + (uint32_t)h) * 256u + (uint32_t)(b & 7) * 16u;
         uint4 xr[kXChunks];
         // with x tiles: the first window goes to the tile the latest window did not use (its MMAs completed
         // before the latest window started); without: windows pass through registers into tile 0
@@ -854,11 +894,11 @@ struct MmaCons {
             const int qc = 8 * p;
             if (qc + 8 <= nq) {
 #pragma unroll
-                for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
+                for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut, kLut256>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
             } else {
 #pragma unroll
                 for (int j = 0; j < 8; j++)
-                    w[j] = (qc + j < nq) ? q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P) : 0u;
+                    w[j] = (qc + j < nq) ? q8_step_t<kWideLut, kLut256>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P) : 0u;
             }
             // the previous pair of MMAs is done with the A tile (and, at a window start, with the x tile)
             wait_mma(L);
@@ -877,7 +917,7 @@ struct MmaCons {
                 // multiplied: the MMAs of a pair read only the pieces that exist)
 #pragma unroll
                 for (int i = 0; i < kXChunks; i++)
-                    asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 512u),
+                    asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 1024u),
                                  "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
                                  : "memory");
                 fence_proxy_async_smem();  // the x tile is read by the tensor core (async proxy)
@@ -890,11 +930,11 @@ struct MmaCons {
                 const int qc2 = qc + 8;
                 if (qc2 + 8 <= nq) {
 #pragma unroll
-                    for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
+                    for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut, kLut256>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 8; j++)
-                        w[j] = (qc2 + j < nq) ? q8_step_t<kWideLut>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P) : 0u;
+                        w[j] = (qc2 + j < nq) ? q8_step_t<kWideLut, kLut256>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P) : 0u;
                 }
                 tmem_st_32x32b_x8_nowait(st_addr + 8u, w);
             }
@@ -914,18 +954,19 @@ struct MmaCons {
 #pragma unroll
             for (int v = 0; v < 16; v++) r[v] = 0;
         }
-        // this warp's MMAs (and x copies) are complete, so its own x tiles take its partial sums:
-        // [vector][stripe row]
-        int *red = xbase + warp * (2 * kXBytes / 4);
+        // this warp's MMAs (and x copies) are complete, so its own x tiles take its partial sums: vector v
+        // of stripe row l at hole (warp's first + v), word l
 #pragma unroll
-        for (int v = 0; v < 16; v++) red[v * 32 + lane] = (int)r[v];
+        for (int v = 0; v < 16; v++)
+            *reinterpret_cast<int *>(sm0 + hole((uint32_t)(hole0 + v)) + 4 * lane) = (int)r[v];
         tcgen05_fence_before();
         __syncthreads();
         const mv_q8_view &m = J.m;
         for (int t = threadIdx.x; t < 16 * 32; t += blockDim.x) {
             const int v = t >> 5, l = t & 31;
             int sum = 0;
-            for (int w = 0; w < W; w++) sum += xbase[w * (2 * kXBytes / 4) + t];
+            for (int w = 0; w < W; w++)
+                sum += *reinterpret_cast<const int *>(sm0 + hole((uint32_t)(w * (int)(2 * kHoles) + v)) + 4 * l);
             const int row = stripe * 32 + l;
             if (row < m.rows && v < L.batch) {
                 int32_t *dst = J.y + (size_t)v * m.rows + row;
@@ -985,6 +1026,7 @@ struct FwdMma {
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
     static constexpr bool kWideLut = false;
+    static constexpr bool kLut256 = false;
     static constexpr int kXPieces = 2;
     static constexpr int kXBytes = kXPieces * 1024;
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
@@ -1159,6 +1201,7 @@ struct BwdMma {
     static constexpr int kMaxThreads = 256;
     static constexpr int kTmemCols = 1;
     static constexpr bool kWideLut = false;
+    static constexpr bool kLut256 = false;
     static constexpr int kGBytes = 4096;  // [hi, lo][K step 0, 1] x 1 KB
     static constexpr int kWBytes = 2048;  // W tile per warp: 2 K steps x 1 KB
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
@@ -1447,7 +1490,8 @@ __device__ __forceinline__ void stage_entries_async(const Q8SLaunch &L, const mv
 
 // Decode table of one item from its staged data (so: relative offsets of the nt + 1 table bounds, tsm: the
 // entries u16 symbol | freq << 8).  Warp w fills quantiles [256 w / W, 256 (w + 1) / W) of every lane column.
-template <bool kWide>
+// Narrow entries sit at word q*kPitch + lane: kPitch 32 (128-byte rows) or 64 (256-byte rows, see MmaCons).
+template <bool kWide, int kPitch = 32>
 __device__ __forceinline__ void build_table(const Q8SLaunch &L, const mv_q8_view &m, uint32_t *lut,
                                             const uint32_t *so, const uint16_t *tsm, int warp, int lane, int W) {
     const int t = m.local ? lane : 0;
@@ -1505,7 +1549,7 @@ __device__ __forceinline__ void build_table(const Q8SLaunch &L, const mv_q8_view
         } else {
             // unrolled: measured 1 % faster for the tensor-core consumer (0.4 % slower for the wide table)
 #pragma unroll 4
-            for (uint32_t q = a; q < e; q++) lut[q * 32 + lane] = f | (sym << 16) | ((q - cum) << 24);
+            for (uint32_t q = a; q < e; q++) lut[q * kPitch + lane] = f | (sym << 16) | ((q - cum) << 24);
         }
         cum += f;
     }
@@ -1514,7 +1558,7 @@ __device__ __forceinline__ void build_table(const Q8SLaunch &L, const mv_q8_view
             if constexpr (kWide)
                 reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(1u, 0u);
             else
-                lut[q * 32 + lane] = 1u;
+                lut[q * kPitch + lane] = 1u;
         }
         atomicOr(L.status, MV_DEV_BAD_TABLE);
     }
@@ -1609,7 +1653,7 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
             } else if (threadIdx.x == 0 && so[36] == 0) {
                 atomicOr(L.status, MV_DEV_BAD_TABLE);
             }
-            build_table<Cons::kWideLut>(L, m, lut, so, se + so[37], warp, lane, W);
+            build_table<Cons::kWideLut, Cons::kLut256 ? 64 : 32>(L, m, lut, so, se + so[37], warp, lane, W);
             fence_proxy_async_smem();  // the table staging may share memory with later bulk copies
             __syncthreads();
             lut_job = I.job;
@@ -1797,7 +1841,7 @@ mv_status launch_q8s_t(const Q8SLaunch &L0, int W, int ctas_per_sm, cudaStream_t
                     Cons::extra_bytes(W));
     Q8SLaunch L = L0;
     auto layout = [&](bool two) {
-        return q8s_layout(Cons::kWideLut ? 256 * 32 * 8 : 256 * 32 * 4, (uint32_t)Cons::extra_bytes(W),
+        return q8s_layout(Cons::kWideLut || Cons::kLut256 ? 256 * 256 : 256 * 32 * 4, (uint32_t)Cons::extra_bytes(W),
                           (uint32_t)Cons::tbl_alias_bytes(W), W, DEPTH, ILP, L.buf_words, Cons::kRedNV,
                           Cons::kRedBufs, L.tbl_stage, two);
     };
@@ -1830,11 +1874,9 @@ mv_status launch_q8s_t(const Q8SLaunch &L0, int W, int ctas_per_sm, cudaStream_t
     }
     if (L.chain_scales) {
         // the chained pipeline waits across CTAs: a cooperative launch guarantees that they are all resident.
-        // The runtime checks the grid against its own occupancy figure, which for tensor-memory kernels is
-        // lower than what the SM holds; a grid it rejects as too large is retried at that figure.
         // The runtime checks the grid against its own occupancy figure (for tensor-memory kernels one CTA
         // per SM, fewer than the SM holds), and a rejected launch would also end a stream capture, so the
-        // grid is taken from that figure; 16-warp CTAs keep a tensor-core chain at 16 warps per SM.
+        // grid is taken from that figure.
         int coop = 0;
         MV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&coop, kern, 32 * W, smem), "occupancy");
         coop = std::max(1, std::min(coop, bps));
@@ -1918,7 +1960,7 @@ mv_q8_tuning resolve(const mv_q8_tuning *t) {
     if (t) {
         if (t->engine == MV_ENGINE_DP4A) r.engine = MV_ENGINE_DP4A;
         if (t->parts > 0) r.parts = t->parts;
-        if (t->warps > 0) r.warps = std::min(16, t->warps);  // more than 8: tensor-core engine only
+        if (t->warps > 0) r.warps = std::min(16, t->warps);  // more than 8: the integer CUDA-core consumer only
         if (t->ilp == 1 || t->ilp == 2) r.ilp = t->ilp;
         if (t->depth == 1 || t->depth == 2) r.depth = t->depth;
         if (t->ctas_per_sm > 0) r.ctas_per_sm = t->ctas_per_sm;

@@ -17,7 +17,7 @@ def test_candidates_per_batch():
     dp4a = [c for c in c16 if c[5] == 1]
     assert mma and dp4a
     assert all(c[1] == 1 for c in mma)                       # the tensor-core engine decodes with ilp 1
-    assert {c[0] for c in mma} == {4, 6, 8, 16}              # up to 16 warps per CTA there
+    assert {c[0] for c in mma} == {4, 6, 8}                  # up to 8 warps per CTA there
     assert sorted(c[:5] for c in dp4a) == sorted(c[:5] for c in base)  # every base candidate on the CUDA cores
     assert len(set(c16)) == len(c16)
 
