@@ -200,9 +200,9 @@ mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int3
                        const float *row_scales_dev, float *y_scaled_dev, void *stream);
 
 /* Launch parameters of the persistent Q8 kernel (0 = library default).
- *   warps        warps per CTA (default 8): up to 16 for the integer
- *                CUDA-core consumer, up to 8 for the tensor-core engine and
- *                the float form
+ *   warps        warps per CTA (default 8; 16 for the float forward on
+ *                the CUDA cores): up to 16, except 8 for the float backward
+ *                and the float form on the tensor cores
  *   ilp          independent segments decoded per warp (1 or 2, default 2;
  *                1 for the float form)
  *   depth        shared-memory stream buffers per warp (1 or 2, default 1):

@@ -479,7 +479,7 @@ struct FwdCons {
     static constexpr int kRedBufs = 1;
     static constexpr bool kFinishSyncs = true;
     static constexpr int kMinCtas = 1;
-    static constexpr int kMaxThreads = 256;
+    static constexpr int kMaxThreads = 512;  // 16 warps: a stripe's segments over more warps (few stripes)
     static constexpr int kTmemCols = 0;
     static constexpr bool kWideLut = true;
     static constexpr bool kLut256 = false;
@@ -728,43 +728,51 @@ __device__ __forceinline__ void BwdCons<NV>::run_step(const Q8SLaunch &L, const 
 //
 // Shared memory: the decode table takes 4-byte entries at a 256-byte pitch
 // (entry (q, lane) at byte q*256 + lane*4, one byte permute per address), and
-// the x tiles live in the other half of each 256-byte row: 256 holes of 128
-// bytes, one core matrix each, 32 per warp (two tiles of 16), hence at most 8
-// warps.  A core matrix (n, k) of piece p of tile t of warp w sits in hole
-// w*32 + t*16 + p*4 + n*2 + k: LBO (K) 256 B, SBO (N) 512 B.  64 KB hold
-// table and x tiles, as much as the 32 KB table with separate x tiles, so two
-// 8-warp CTAs still fit an SM.  The holes also take the cross-warp reduction.
+// the x tiles of warps 0..7 live in the other half of each 256-byte row: 256
+// holes of 128 bytes, one core matrix each, 32 per warp (two tiles of 16).
+// Core matrix c = t*16 + p*4 + n*2 + k ((n, k) of piece p of tile t) sits at
+// base + c * stride: stride 256 B in the holes (LBO, K direction, 256 B; SBO,
+// N direction, 512 B), 128 B for warps 8..15, whose tiles are contiguous
+// behind the table (LBO 128, SBO 256).  64 KB hold table and eight warps' x
+// tiles, as much as the 32 KB table with separate x tiles, so two 8-warp CTAs
+// still fit an SM.  The tiles also take the cross-warp reduction.
 struct MmaCons {
     static constexpr int kNV = 16;
     static constexpr int kRedNV = 0;      // reduction area: the x tiles
     static constexpr int kRedBufs = 1;
     static constexpr bool kFinishSyncs = true;
-    static constexpr int kMinCtas = 2;    // at most 128 registers per thread
-    static constexpr int kMaxThreads = 256;  // 32 holes per warp
+    static constexpr int kMinCtas = 1;    // with up to 16 warps: at most 128 registers per thread
+    static constexpr int kMaxThreads = 512;  // 2 x 8 warps per SM (stacks) or 1 x 16 (chains)
     static constexpr int kTmemCols = 1;   // > 0: the kernel allocates TMEM
     static constexpr bool kWideLut = false;
     static constexpr bool kLut256 = true;  // 4-byte entries at a 256-byte pitch, x tiles in between
     static constexpr int kXChunks = 4;    // x tile: 4 pieces of 32 columns x 16 vectors (512 B each)
     static constexpr int kXBytes = kXChunks * 512;
     static constexpr uint32_t kHoles = kXBytes / 128;  // core matrices per tile
+    // x tiles of warps 8..15 (4 KB each) at the start of the consumer region
+    static __host__ __device__ constexpr size_t xr_bytes(int W) { return W > 8 ? (size_t)(W - 8) * 2 * kXBytes : 0; }
     static __host__ __device__ constexpr size_t extra_bytes(int W) {
-        // three mbarriers per warp (MMA commits, x copies into tile 0 / 1), TMEM address slot (the last 128
-        // bytes); a multiple of 128 bytes, so the stream buffers that follow stay 16-byte aligned
-        return (((size_t)W * 24 + 128) + 127) / 128 * 128;
+        // those x tiles, three mbarriers per warp (MMA commits, x copies into tile 0 / 1), TMEM address slot
+        // (the last 128 bytes); a multiple of 128 bytes, so the stream buffers that follow stay 16-byte
+        // aligned
+        return ((xr_bytes(W) + (size_t)W * 24 + 128) + 127) / 128 * 128;
     }
     static __host__ __device__ constexpr size_t tbl_alias_bytes(int) { return 0; }
     static __host__ __device__ constexpr uint32_t tmem_cols(int W) {
         return W <= 1 ? 32 : W <= 2 ? 64 : W <= 4 ? 128 : W <= 8 ? 256 : 512;
     }
-    // hole h: byte h*256 + 128 from the start of shared memory
-    static __device__ __forceinline__ uint32_t hole(uint32_t h) { return h * 256u + 128u; }
-    uint32_t xt, d_tmem, st_addr, ld_addr, ncommit, xcur, xcnt0, xcnt1;
+    // warp w's core matrix 0 of tile 0 (byte offset from the start of shared memory) and core-matrix stride
+    static __device__ __forceinline__ uint32_t tile_base(const Q8SLaunch &L, int w) {
+        return w < 8 ? (uint32_t)w * (2u * kHoles) * 256u + 128u : L.lay.extra + (uint32_t)(w - 8) * 2u * kXBytes;
+    }
+    static __device__ __forceinline__ uint32_t tile_stride(int w) { return w < 8 ? 256u : 128u; }
+    uint32_t xt, d_tmem, st_addr, ld_addr, ncommit, xcur, xcnt0, xcnt1, xb, cst;
     uint64_t b_desc0;
     uint64_t *mbar, *xbar;
     unsigned char *sm0;  // start of shared memory (table and holes)
     const int8_t *x;
     const int8_t *tiles;  // x laid out per (segment, window) by q8s_build_x_tiles, or null
-    int cols, batch, job_idx, nwin, hole0;
+    int cols, batch, job_idx, nwin;
     bool any;
 
     __device__ __forceinline__ void init(const Q8SLaunch &L, unsigned char *extra, uint32_t tmem_base, int,
@@ -773,10 +781,11 @@ struct MmaCons {
         // operands derived from it stay in uniform registers
         const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
         sm0 = extra - L.lay.extra;  // the table (and its holes) starts shared memory
-        hole0 = warp * (int)(2 * kHoles);
-        xt = smem_u32(sm0) + hole((uint32_t)hole0);  // tile 0, core matrix 0
-        mbar = reinterpret_cast<uint64_t *>(extra) + warp;
-        xbar = reinterpret_cast<uint64_t *>(extra + (size_t)W * 8) + 2 * warp;
+        xb = tile_base(L, warp);
+        cst = tile_stride(warp);
+        xt = smem_u32(sm0) + xb;  // tile 0, core matrix 0
+        mbar = reinterpret_cast<uint64_t *>(extra + xr_bytes(W)) + warp;
+        xbar = reinterpret_cast<uint64_t *>(extra + xr_bytes(W) + (size_t)W * 8) + 2 * warp;
         if (lane == 0) {
             mbar_init(mbar, 1);
             mbar_init(&xbar[0], 1);
@@ -790,7 +799,7 @@ struct MmaCons {
         d_tmem = tmem_base + 32u * (uint32_t)warp;
         st_addr = d_tmem + 16u + quarter;
         ld_addr = d_tmem + quarter;
-        b_desc0 = umma_smem_desc(xt, 256u, 512u);
+        b_desc0 = umma_smem_desc(xt, cst, 2u * cst);
         ncommit = 0;
         xcur = 1;  // the x tile of the latest window; a segment's first window goes to the other one
         xcnt0 = xcnt1 = 0;
@@ -812,7 +821,7 @@ struct MmaCons {
         if (lane == 0) mbar_arrive_expect_tx(&xbar[t], (uint32_t)kXBytes);
         __syncwarp();
         if (lane < (int)kHoles)
-            bulk_g2s(sm0 + hole((uint32_t)(hole0 + t * (int)kHoles + lane)),
+            bulk_g2s(sm0 + xb + ((uint32_t)t * kHoles + (uint32_t)lane) * cst,
                      tiles + ((size_t)seg * nwin + w) * kXBytes + (size_t)lane * 128, 128u, &xbar[t]);
         if (t) xcnt1++;
         else xcnt0++;
@@ -833,12 +842,11 @@ struct MmaCons {
         __syncwarp();
         if (elect_one()) {
             tcgen05_fence_after();
-            // B descriptor start addresses are in 16-byte units: tile xcur is 16 holes (4 KB) in, piece p 4
-            // holes (1 KB)
+            // B descriptor start addresses are in 16-byte units: tile xcur is 16 core matrices in, piece p 4
             const uint32_t idesc = umma_idesc_i8(128, 16);
-            const uint64_t bd = b_desc0 + (uint64_t)(xcur * (kHoles * 16) + piece * 64);
+            const uint64_t bd = b_desc0 + (uint64_t)(xcur * cst + (uint32_t)piece * (cst / 4u));
             umma_i8_ts(d_tmem, d_tmem + 16u, bd, idesc, any ? 1u : 0u);
-            if (two) umma_i8_ts(d_tmem, d_tmem + 24u, bd + 64u, idesc, 1u);  // the next piece, 1 KB on
+            if (two) umma_i8_ts(d_tmem, d_tmem + 24u, bd + cst / 4u, idesc, 1u);  // the next piece
             umma_commit(mbar);
         }
         __syncwarp();
@@ -875,8 +883,8 @@ struct MmaCons {
         const bool xok = b < batch;
         const int colbase = 4 * q0 + 16 * h;
         const int8_t *xrow = x + (size_t)(xok ? b : 0) * cols + colbase;
-        // core matrix (n, k) = (b / 8, h) of piece i in hole 4 i + 2 n + k of tile 0, row b % 8
-        const uint32_t xdst = xt + ((uint32_t)(b >> 3) * 2u + (uint32_t)h) * 256u + (uint32_t)(b & 7) * 16u;
+        // core matrix (n, k) = (b / 8, h) of piece i is core matrix 4 i + 2 n + k of tile 0, row b % 8
+        const uint32_t xdst = xt + ((uint32_t)(b >> 3) * 2u + (uint32_t)h) * cst + (uint32_t)(b & 7) * 16u;
         uint4 xr[kXChunks];
         // with x tiles: the first window goes to the tile the latest window did not use (its MMAs completed
         // before the latest window started); without: windows pass through registers into tile 0
@@ -917,7 +925,7 @@ struct MmaCons {
                 // multiplied: the MMAs of a pair read only the pieces that exist)
 #pragma unroll
                 for (int i = 0; i < kXChunks; i++)
-                    asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 1024u),
+                    asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(xdst + (uint32_t)i * 4u * cst),
                                  "r"(xr[i].x), "r"(xr[i].y), "r"(xr[i].z), "r"(xr[i].w)
                                  : "memory");
                 fence_proxy_async_smem();  // the x tile is read by the tensor core (async proxy)
@@ -955,10 +963,9 @@ struct MmaCons {
             for (int v = 0; v < 16; v++) r[v] = 0;
         }
         // this warp's MMAs (and x copies) are complete, so its own x tiles take its partial sums: vector v
-        // of stripe row l at hole (warp's first + v), word l
+        // of stripe row l in core matrix v of tile 0, word l
 #pragma unroll
-        for (int v = 0; v < 16; v++)
-            *reinterpret_cast<int *>(sm0 + hole((uint32_t)(hole0 + v)) + 4 * lane) = (int)r[v];
+        for (int v = 0; v < 16; v++) *reinterpret_cast<int *>(sm0 + xb + (uint32_t)v * cst + 4 * lane) = (int)r[v];
         tcgen05_fence_before();
         __syncthreads();
         const mv_q8_view &m = J.m;
@@ -966,7 +973,7 @@ struct MmaCons {
             const int v = t >> 5, l = t & 31;
             int sum = 0;
             for (int w = 0; w < W; w++)
-                sum += *reinterpret_cast<const int *>(sm0 + hole((uint32_t)(w * (int)(2 * kHoles) + v)) + 4 * l);
+                sum += *reinterpret_cast<const int *>(sm0 + tile_base(L, w) + (uint32_t)v * tile_stride(w) + 4 * l);
             const int row = stripe * 32 + l;
             if (row < m.rows && v < L.batch) {
                 int32_t *dst = J.y + (size_t)v * m.rows + row;
@@ -2097,6 +2104,11 @@ mv_status mv_q8_matvec_bf16(const mv_q8_view *m, const uint16_t *x_dev, int batc
     mv_q8_tuning t = mv::resolve(tuning);
     t.parts = 1;
     if (!tuning || (tuning->ilp != 1 && tuning->ilp != 2)) t.ilp = 1;  // the float form's default
+    // the forward keeps whole stripes per item (a fixed-order reduction): with fewer stripes than SMs, the
+    // CUDA-core consumer takes 16-warp CTAs so that each stripe's segments spread over more warps
+    // (4096x11008, one vector: 35.0 against 43.2 us; with 344 stripes 8 warps stay faster, 43.2 against 47.3)
+    if ((!tuning || tuning->warps <= 0) && mv::q8f_pass(1, batch, t) <= 8 && (m->rows + 31) / 32 < mv::sm_count())
+        t.warps = 16;
     return mv::q8f_run(m, 1, x_dev, batch, row_scales_dev, y_dev, &t, (cudaStream_t)stream);
 }
 

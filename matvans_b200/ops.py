@@ -358,8 +358,8 @@ class Q8Chain:
         if len(scales) != len(self.matrices):
             raise ValueError("one scale per matrix")
         # a chain launch is cooperative (one CTA per SM on the tensor cores) and each step's work items are
-        # whole stripes: 16-warp CTAs give each stripe the most warps (8 on the tensor cores, their limit)
-        default = (16, 1, 1, 0) if self.batch < 5 else (8, 1, 1, 0)
+        # whole stripes: 16-warp CTAs give each stripe the most warps
+        default = (16, 1, 1, 0)
         self.tuning = tuning if isinstance(tuning, Q8Tuning) else Q8Tuning(*(tuning or default))
         self.scales = torch.tensor([float(s) for s in scales], dtype=torch.float32, device=self.device)
         self.xs = [x0 if x0 is not None else torch.zeros((self.batch, self.matrices[0].cols), dtype=torch.int8,

@@ -30,8 +30,8 @@ def clean_status():
 def _both_engines(M, W, x, s, tuning):
     t = tuple(tuning) + (0,) * (5 - len(tuning))
     xt = torch.from_numpy(x)
-    # both engines take at most 8 warps per CTA here (the tensor-core one: 32 x-tile holes per warp in 64 KB)
-    y0, ys0 = M.matvec(xt, scales=s, tuning=(min(t[0], 8),) + t[1:] + (MMA,))
+    y0, ys0 = M.matvec(xt, scales=s, tuning=t + (MMA,))
+    # the CUDA-core engine takes at most 8 warps per CTA
     y1, ys1 = M.matvec(xt, scales=s, tuning=(min(t[0], 8),) + t[1:] + (DP4A,))
     yref = oracle.matvec_i8(W, x)
     assert np.array_equal(y0.cpu().numpy(), yref)
@@ -63,7 +63,8 @@ def test_mma_segment_lengths(seg_quads):
     s = rng.uniform(1e-3, 1e-2, size=96).astype(np.float32)
     tunings = [(1, 1, 1, 0), (4, 1, 2, 0), (8, 1, 1, 0, 3), (3, 1, 2, 2)]
     if seg_quads <= 64:  # 8 warps of two 128-quad stream buffers exceed shared memory (rejected, tested below)
-        tunings += [(8, 1, 2, 0), (6, 1, 2, 0, 2)]
+        # 16 warps: warps 8..15 keep their x tiles outside the decode table's holes
+        tunings += [(8, 1, 2, 0), (6, 1, 2, 0, 2), (16, 1, 1, 0), (12, 1, 1, 0, 2)]
     for tuning in tunings:
         _both_engines(M, W, x, s, tuning)
     assert ops.device_status() == 0
@@ -71,14 +72,14 @@ def test_mma_segment_lengths(seg_quads):
 
 def test_launches_that_do_not_fit_are_rejected():
     M = ops.Q8Matrix.encode(np.ones((64, 512), np.int8))
-    with pytest.raises(_lib.MatvansError):  # the CUDA-core float consumers take at most 8 warps per CTA
-        M.matvec_bf16(torch.ones((1, 512), dtype=torch.bfloat16, device="cuda"),
-                      torch.ones(64, device="cuda"), tuning=(16, 1, 1, 0, 0, DP4A))
+    with pytest.raises(_lib.MatvansError):  # the CUDA-core float backward takes at most 8 warps per CTA
+        M.matvec_t_bf16(torch.ones((1, 64), dtype=torch.bfloat16, device="cuda"),
+                        torch.ones(64, device="cuda"), tuning=(16, 1, 1, 0, 0, DP4A))
     W = np.random.default_rng(1).integers(-127, 128, size=(96, 1520)).astype(np.int8)  # ~8 bits/weight
     M = ops.Q8Matrix.encode(W, local=True, seg_quads=128)
     with pytest.raises(_lib.MatvansError):  # 8 warps of two 128-quad stream buffers exceed shared memory
         M.matvec(torch.ones((16, 1520), dtype=torch.int8), tuning=(8, 1, 2, 0, 0, MMA))
-    with pytest.raises(_lib.MatvansError):  # the tensor-core engine takes at most 8 warps per CTA
+    with pytest.raises(_lib.MatvansError):  # so do 16 warps of one 128-quad stream buffer each
         M.matvec(torch.ones((16, 1520), dtype=torch.int8), tuning=(16, 1, 1, 0, 0, MMA))
     assert ops.device_status() == 0
 
