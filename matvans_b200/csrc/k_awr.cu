@@ -58,13 +58,17 @@ __global__ void __launch_bounds__(256) awr_kernel(const AwrLaunch L) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
     const int nq = L.cols >> 2;
 
-    for (int i = threadIdx.x; i < 128 * 32; i += blockDim.x) {
-        const uint32_t q = (uint32_t)i >> 5, sh = 8 * (q & 3);
+    // one entry per quantile (its table reads once), written to all 32 lane columns with a rotating column
+    // index so that a half-warp's 8-byte stores hit distinct banks
+    for (uint32_t q = threadIdx.x; q < 128; q += blockDim.x) {
+        const uint32_t sh = 8 * (q & 3);
         const uint32_t sym = (__ldg(L.ppf + (q >> 2)) >> sh) & 0xFF;
         const uint32_t c = (__ldg(L.cum + (q >> 2)) >> sh) & 0xFF;
         const uint32_t p = (__ldg(L.prob + (q >> 2)) >> sh) & 0xFF;
         if (c > q || p == 0) atomicOr(L.status, MV_DEV_BAD_TABLE);
-        lut[i] = make_uint2(p | (sym << 16), (q - c) & 0xFFFFu);
+        const uint2 e = make_uint2(p | (sym << 16), (q - c) & 0xFFFFu);
+#pragma unroll 8
+        for (uint32_t l = 0; l < 32; l++) lut[q * 32 + ((l + q) & 31)] = e;
     }
     const bool xal = (reinterpret_cast<uintptr_t>(L.x) & 3) == 0;
     for (int i = threadIdx.x; i < nq * NV; i += blockDim.x) {

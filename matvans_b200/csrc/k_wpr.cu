@@ -7,10 +7,10 @@
 // r = ppf[q], w = min + r, head = (head >> 8) * prob(r) + (q - cdf[r]), refill
 // 16 bits when head < 2^16 (kernel.cu:120-157).  B200 changes: the reference's
 // per-lane 16-entry ring queue in local memory (kernel.cu:3-44) becomes one
-// prefetched register word; cdf/ppf become one 256 x 32-lane conflict-free
-// shared table of packed (symbol, prob, q - cdf) entries; four decoded
-// symbols go through one dp4a instead of four scalar multiplies; any number of
-// vectors share a decode.
+// prefetched register word, refilled by selects (no divergent branch);
+// cdf/ppf become one 256 x 32-lane conflict-free shared table of packed
+// (symbol, prob, q - cdf) entries; four decoded symbols go through one dp4a
+// instead of four scalar multiplies; any number of vectors share a decode.
 #include <algorithm>
 
 #include "mv_device.cuh"
@@ -41,8 +41,9 @@ __global__ void __launch_bounds__(256) wpr_kernel(const WprLaunch L) {
     uint8_t *xs = reinterpret_cast<uint8_t *>(lut + 256 * 32);  // [NV][cols]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
 
-    for (int i = threadIdx.x; i < 256 * 32; i += blockDim.x) {
-        const uint32_t q = (uint32_t)i >> 5;
+    // one entry per quantile (its three table reads once), written to all 32 lane columns with a rotating
+    // column index so that a warp's stores hit 32 different banks
+    for (uint32_t q = threadIdx.x; q < 256; q += blockDim.x) {
         const uint32_t r = __ldg(L.ppf + q);
         uint32_t e = 0;
         if ((int)r + 1 > L.G) {
@@ -54,7 +55,8 @@ __global__ void __launch_bounds__(256) wpr_kernel(const WprLaunch L) {
             if (c0 > q) atomicOr(L.status, MV_DEV_BAD_TABLE);
             e = (uint32_t)(uint8_t)(int8_t)(L.min_value + (int)r) | (prob << 8) | ((bias & 0xFFFF) << 16);
         }
-        lut[i] = e;
+#pragma unroll 8
+        for (uint32_t l = 0; l < 32; l++) lut[q * 32 + ((l + q) & 31)] = e;
     }
     for (int i = threadIdx.x; i < NV * L.cols / 16; i += blockDim.x) {
         const int v = i / (L.cols / 16);
@@ -66,20 +68,28 @@ __global__ void __launch_bounds__(256) wpr_kernel(const WprLaunch L) {
 
     const uint32_t *lut_l = lut + lane;
     const int steps = L.cols / 32;
+    const uint32_t size = (uint32_t)L.payload_size;  // < 0xF0000000 (checked by the launcher)
     for (int row = blockIdx.x * W + warp; row < L.rows; row += gridDim.x * W) {
-        const size_t cursor = __ldg(L.cursors + row);
-        const uint16_t *base = L.payload + cursor + 8 * lane;
-        bool ovf = false, nw_oob = false;
-        auto fetch = [&](uint32_t k, bool &oob) -> uint32_t {
-            const size_t idx = cursor + (size_t)(k >> 3) * 256 + 8 * lane + (k & 7);
-            oob = idx >= L.payload_size;
-            return oob ? 0u : (uint32_t)__ldg(base + (size_t)(k >> 3) * 256 + (k & 7));
-        };
-        bool oob0, oob1;
-        uint32_t head = (fetch(0, oob0) << 16) | fetch(1, oob1);
-        ovf = oob0 || oob1;
-        uint32_t k = 2;
-        uint32_t nw = fetch(k, nw_oob);
+        // The lane's word k sits at ix = cursor + (k / 8) * 256 + 8 * lane + k % 8: ix advances by 1 inside a
+        // group of 8 words and by 249 from one group to the next.  Reads past the payload return 0 and are
+        // flagged (a cursor past the payload starts the lane at its end; ix then grows by at most 249 per
+        // symbol, far below 2^32 from a payload under 0xF0000000 words).  Two words are in flight ahead of
+        // the state, so a fetch's latency is covered by the symbols of two refills; the refill itself is
+        // selects, not a branch, because the lanes refill at different steps.
+        const uint64_t ix0 = (uint64_t)__ldg(L.cursors + row) + 8u * (uint32_t)lane;
+        uint32_t ix = ix0 < size ? (uint32_t)ix0 : size;
+        bool ovf = (uint64_t)ix + 2u > size;
+        const uint32_t w0 = ix < size ? (uint32_t)__ldg(L.payload + ix) : 0u;
+        const uint32_t w1 = ix + 1u < size ? (uint32_t)__ldg(L.payload + ix + 1u) : 0u;
+        uint32_t head = (w0 << 16) | w1;
+        // two words in flight: nw (word k) and nw2 (word k + 1, at ix)
+        ix += 2u;
+        bool nw_oob = ix >= size;
+        uint32_t nw = nw_oob ? 0u : (uint32_t)__ldg(L.payload + ix);
+        ix += 1u;
+        uint32_t j = 3;  // ix's position inside its group of 8
+        bool nw2_oob = ix >= size;
+        uint32_t nw2 = nw2_oob ? 0u : (uint32_t)__ldg(L.payload + ix);
         int acc[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = 0;
@@ -90,19 +100,25 @@ __global__ void __launch_bounds__(256) wpr_kernel(const WprLaunch L) {
             for (int v = 0; v < NV; v++) xv[v] = *reinterpret_cast<const uint4 *>(xs + (size_t)v * L.cols + colbase);
 #pragma unroll
             for (int g = 0; g < 4; g++) {
-                uint32_t wq = 0;
+                uint32_t e[4];
 #pragma unroll
                 for (int t = 0; t < 4; t++) {
-                    const uint32_t q = head & 0xFF;
-                    const uint32_t e = lut_l[q << 5];
-                    wq |= (e & 0xFF) << (8 * t);
-                    head = (head >> 8) * __byte_perm(e, 0, 0x4441) + (e >> 16);
-                    if (head < (1u << 16)) {
-                        head = (head << 16) | nw;
-                        ovf |= nw_oob;
-                        nw = fetch(++k, nw_oob);
+                    e[t] = lut_l[(head & 0xFFu) << 5];
+                    head = (head >> 8) * __byte_perm(e[t], 0, 0x4441) + (e[t] >> 16);
+                    const bool need = head < (1u << 16);
+                    head = need ? __byte_perm(nw, head, 0x5410) : head;  // (head << 16) | nw
+                    ovf |= need & nw_oob;
+                    if (need) {
+                        nw = nw2;
+                        nw_oob = nw2_oob;
+                        ix += j == 7u ? 249u : 1u;
+                        j = (j + 1u) & 7u;
+                        nw2_oob = ix >= size;
+                        nw2 = nw2_oob ? 0u : (uint32_t)__ldg(L.payload + ix);
                     }
                 }
+                // the four symbols (byte 0 of each entry) packed in column order
+                const uint32_t wq = __byte_perm(__byte_perm(e[0], e[1], 0x0040), __byte_perm(e[2], e[3], 0x0040), 0x5410);
 #pragma unroll
                 for (int v = 0; v < NV; v++) {
                     const uint32_t xw = g == 0 ? xv[v].x : g == 1 ? xv[v].y : g == 2 ? xv[v].z : xv[v].w;
@@ -180,6 +196,7 @@ mv_status wpr_matvec(const uint16_t *payload, size_t payload_size, const uint32_
     if (((uintptr_t)payload & 15) || ((uintptr_t)x & 15))
         return fail(MV_ERR_ARG, "mv_wpr_matvec: payload and x must be 16-byte aligned");
     if (ys && !scales) return fail(MV_ERR_ARG, "mv_wpr_matvec: y_scaled needs row scales");
+    if (payload_size >= 0xF0000000u) return fail(MV_ERR_UNSUPPORTED, "mv_wpr_matvec: payload of 0xF0000000 words or more");
     mv_status rc;
     WprLaunch L{};
     L.status = device_status_word(&rc);
