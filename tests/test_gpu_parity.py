@@ -297,6 +297,19 @@ def test_wpr_corrupt_payload_is_reported():
     assert ops.device_status(raise_on_error=False) & _lib.DEV_FINAL_STATE
 
 
+def test_wpr_cursors_past_payload_are_reported():
+    # a row whose cursor points past the payload (or near 2^32) reads zeros and raises the overrun flag
+    f = formats.read_wpr_bin(golden("wpr_c1_1024.bin"))
+    m = f["matrices"][0]
+    for bad in (m["payload"].size + 5, 0xFFFFFF00):
+        cur = m["cursors"].copy()
+        cur[7] = bad
+        M = ops.WprMatrix(codec.CompressedMatrix(1024, 1024, 1.0, cur, m["min_value"], m["cdf"], m["ppf"],
+                                                 m["payload"]))
+        M.matvec(torch.from_numpy(f["vector"]))
+        assert ops.device_status(raise_on_error=False) & _lib.DEV_STREAM_OVERRUN
+
+
 def test_bounded_wait_times_out_with_status():
     rng = np.random.default_rng(13)
     W = gauss(rng, 4.0, (64, 512))
