@@ -326,7 +326,7 @@ def chain_section(torch, ops, autotune, dev, mats, batches=(1, 16), reps=5, scal
 
 
 def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, reps=10):
-    """configs: the 224-matrix uneven stack, one persistent launch per step, B in {1,4,8,16}; the tensor-core
+    """The 224-matrix uneven stack, one persistent launch per step, B in {1,4,8,16}; the tensor-core
     engine competes with dp4a at B >= 8.  Gate: bit-exact against the dense int8 kernel on the same x."""
     t_build = time.perf_counter()
     mats = build_stack(torch, ops, dev, layers)
@@ -430,7 +430,7 @@ def int8_gemm_us(torch, Ws, x, reps=10):
 
 
 def large_section(torch, ops, autotune, dev, batches=(1, 16)):
-    """configs: 16384x16384 and 28672x8192, Laplace(b=2) and round(N(0,1)), per-row tables, B in {1, 16}:
+    """Large low-entropy matrices: 16384x16384 and 28672x8192, Laplace(b=2) and round(N(0,1)), per-row tables, B in {1, 16}:
     us per matvec of the autotuned single launch and of dense dp4a, bits/weight vs entropy, HBM GB/s."""
     from matvans_b200 import codec
     out = {}
@@ -865,7 +865,7 @@ def run_ours(args):
     ref_kernels = reference_kernels_section(torch, ops, dev, mats, xd, {k: v["us"] for k, v in per.items()}) \
         if extras else None
 
-    # float form (configs[3] shapes): forward and re-decoding backward, us per call
+    # float form (4096x11008 and 11008x4096, sigma 4, per-row scales): forward and re-decoding backward, us per call
     float_form = {}
     for m in (mats if extras else []):
         if m["sigma"] != 4.0 or m["shape"] == (4096, 4096):
