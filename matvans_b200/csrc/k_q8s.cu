@@ -1413,7 +1413,7 @@ __global__ void q8s_chain_reset(Q8Job *jobs, int njobs) {
 // Shared-memory layout of q8s_kernel (byte offsets), computed on the host and passed with the launch.
 __host__ __device__ inline Q8SLayout q8s_layout(uint32_t lut_bytes, uint32_t extra_bytes, uint32_t tbl_alias, int W,
                                                 int DEPTH, int ILP, int buf_words, int red_nv, int red_bufs,
-                                                int tbl_stage, bool two_areas = true) {
+                                                int tbl_stage) {
     Q8SLayout o{};
     uint32_t p = lut_bytes;
     o.extra = p;
@@ -1432,21 +1432,23 @@ __host__ __device__ inline Q8SLayout q8s_layout(uint32_t lut_bytes, uint32_t ext
     o.sched = p;  // scheduler state (thread 0)
     p += (uint32_t)sizeof(SchedState);
     p = (p + 15u) & ~15u;
-    o.stage_o = p;  // [2][kStageOffs]
-    p += 2u * kStageOffs * 4u;
+    o.stage_o = p;  // [kStageOffs]
+    p += kStageOffs * 4u;
     o.rows = p;  // [W][DEPTH][ILP] word-rows of each slot's blocks
     p += (uint32_t)(W * DEPTH * ILP) * 4u;
     p = (p + 15u) & ~15u;
-    // table staging: two areas (staged one item ahead, asynchronously), or one inside the consumer's region
-    // when that is free at table rebuilds and large enough, or one area of its own (staged synchronously)
+    // table staging: one area of its own, staged one item ahead asynchronously (the next item's data goes in
+    // only after the current item's table build and the barrier behind it, so one area serves both), or,
+    // staged synchronously, one inside the consumer's region when that is free at table rebuilds and large
+    // enough
     const uint32_t stage_bytes = ((uint32_t)tbl_stage + kStagePad) * 2u;
     o.async_tables = 0;
     if (tbl_alias >= stage_bytes) {
         o.stage_e = o.extra;
     } else {
         o.stage_e = p;
-        o.async_tables = two_areas ? 1u : 0u;
-        p += (two_areas ? 2u : 1u) * stage_bytes;
+        o.async_tables = 1;
+        p += stage_bytes;
     }
     o.total = p;
     return o;
@@ -1622,7 +1624,8 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
 
     // decode table at the start of shared memory: 256 quantiles x 32 lanes of 4 B (narrow) or 8 B (wide); the
     // rest of the layout comes with the launch (L.lay), so its offsets are constant-bank operands.
-    // Two staging areas: the next item's table data is staged while the current item decodes.
+    // Asynchronous table staging: the next item's table data is staged (into the one staging area, after this
+    // item's table build and its barrier) while the current item decodes.
     const bool async_tbl = L.lay.async_tables != 0;
     uint32_t *lut = reinterpret_cast<uint32_t *>(smem);
     unsigned char *extra = smem + L.lay.extra;
@@ -1688,13 +1691,12 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
         if (I.it < 0) break;
         const Q8Job &J = job_at(L, I.job);
         const mv_q8_view &m = J.m;
-        const uint32_t area = async_tbl ? (uint32_t)(k & 1) : 0u;
 
         // decode table, rebuilt only when it changes (uniform across the CTA).  Every warp finished the
         // previous item's decode before the CTA barrier that ended it.
         if (I.job != lut_job || (m.local && I.stripe != lut_stripe)) {
-            uint32_t *so = reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + area * kStageOffs;
-            uint16_t *se = reinterpret_cast<uint16_t *>(smem + L.lay.stage_e) + area * L.stage_len;
+            uint32_t *so = reinterpret_cast<uint32_t *>(smem + L.lay.stage_o);
+            uint16_t *se = reinterpret_cast<uint16_t *>(smem + L.lay.stage_e);
             if (!async_tbl || k == 0) {
                 __syncthreads();  // the staging area may be the consumer's region
                 stage_table_sync(L, m, I.stripe, so, se);
@@ -1726,8 +1728,7 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
             if (N.it >= 0) {
                 const mv_q8_view &mn = job_at(L, N.job).m;
                 if (N.job != I.job || (mn.local && N.stripe != I.stripe)) {
-                    stage_offsets_async(mn, N.stripe, lane,
-                                        reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + (area ^ 1u) * kStageOffs);
+                    stage_offsets_async(mn, N.stripe, lane, reinterpret_cast<uint32_t *>(smem + L.lay.stage_o));
                     pf_state = 1;
                 }
             }
@@ -1777,15 +1778,15 @@ __global__ void __launch_bounds__(Cons::kMaxThreads, Cons::kMinCtas) q8s_kernel(
             issued = __shfl_sync(0xffffffffu, issued, 0);
             if (pf_state == 1) {  // staging warp, second phase (after its first step): the entries
                 stage_entries_async(L, job_at(L, ring[(k + 1) % kRing].job).m, lane,
-                                    reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + (area ^ 1u) * kStageOffs,
-                                    reinterpret_cast<uint16_t *>(smem + L.lay.stage_e) + (area ^ 1u) * L.stage_len);
+                                    reinterpret_cast<uint32_t *>(smem + L.lay.stage_o),
+                                    reinterpret_cast<uint16_t *>(smem + L.lay.stage_e));
                 pf_state = 2;
             }
         }
         if (pf_state == 1)
             stage_entries_async(L, job_at(L, ring[(k + 1) % kRing].job).m, lane,
-                                reinterpret_cast<uint32_t *>(smem + L.lay.stage_o) + (area ^ 1u) * kStageOffs,
-                                reinterpret_cast<uint16_t *>(smem + L.lay.stage_e) + (area ^ 1u) * L.stage_len);
+                                reinterpret_cast<uint32_t *>(smem + L.lay.stage_o),
+                                reinterpret_cast<uint16_t *>(smem + L.lay.stage_e));
         if (pf_state) cp_async_wait_all();  // visible to the CTA after the barrier that ends the item
         if (threadIdx.x == 0 && sch->grab_now) {  // record item k + 2
             SchedState st = *sch;
@@ -1889,19 +1890,9 @@ mv_status launch_q8s_t(const Q8SLaunch &L0, int W, int ctas_per_sm, cudaStream_t
         return fail(MV_ERR_UNSUPPORTED, "Q8 stack launch: consumer region of %zu B breaks 16-byte alignment",
                     Cons::extra_bytes(W));
     Q8SLaunch L = L0;
-    auto layout = [&](bool two) {
-        return q8s_layout(Cons::kWideLut || Cons::kLut256 ? 256 * 256 : 256 * 32 * 4, (uint32_t)Cons::extra_bytes(W),
-                          (uint32_t)Cons::tbl_alias_bytes(W), W, DEPTH, ILP, L.buf_words, Cons::kRedNV,
-                          Cons::kRedBufs, L.tbl_stage, two);
-    };
-    L.lay = layout(true);
-    {
-        // asynchronous table staging needs a second area: keep it only if it costs no resident CTA
-        const Q8SLayout one = layout(false);
-        const int per_sm = max_smem_per_sm(), reserved = 1024;
-        if (L.lay.async_tables && per_sm / (int)(L.lay.total + reserved) < per_sm / (int)(one.total + reserved))
-            L.lay = one;
-    }
+    L.lay = q8s_layout(Cons::kWideLut || Cons::kLut256 ? 256 * 256 : 256 * 32 * 4, (uint32_t)Cons::extra_bytes(W),
+                       (uint32_t)Cons::tbl_alias_bytes(W), W, DEPTH, ILP, L.buf_words, Cons::kRedNV, Cons::kRedBufs,
+                       L.tbl_stage);
     L.slot_bytes = (uint32_t)ILP * (uint32_t)L.buf_words * 4u;
     L.stage_len = (uint32_t)L.tbl_stage + kStagePad;
     const size_t smem = L.lay.total;
