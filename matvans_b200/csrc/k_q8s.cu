@@ -830,8 +830,8 @@ struct MmaCons {
         xbar = reinterpret_cast<uint64_t *>(extra + xr_bytes(W) + (size_t)W * 8) + 2 * warp;
         if (lane == 0) {
             mbar_init(mbar, 1);
-            mbar_init(&xbar[0], 1);
-            mbar_init(&xbar[1], 1);
+            mbar_init(&xbar[0], 32);  // x windows: one arrival per lane (x_copy)
+            mbar_init(&xbar[1], 32);
         }
         fence_mbar_init();
         __syncwarp();
@@ -855,24 +855,32 @@ struct MmaCons {
         tiles = J.x_tiles;
         nwin = (J.m.seg_quads + 31) / 32;
     }
-    // Bulk copies (async proxy) of x window w of segment seg into tile t: lane c < 16 copies core matrix c
-    // (128 bytes) into its hole; lane 0 announces the 2 KB first.  Every lane counts the window.  The
-    // tile's previous readers (MMAs) are done, and generic writes to it (reduction area) were fenced by
-    // every writer before the CTA barrier that ended them.
+    // Asynchronous copies of x window w of segment seg (2 KB, contiguous in the x tiles) into tile t: lane l
+    // copies the 16-byte rows l, l + 32, l + 64, l + 96 (row k = row k % 8 of core matrix k / 8, which sits in
+    // its own hole) and then arrives on the tile's barrier once its copies have landed.  Every lane counts
+    // the window.  The tile's previous readers (MMAs) are done.  Per-lane 16-byte copies rather than one
+    // 128-byte bulk copy per core matrix: bulk copies take warp-uniform operands, so sixteen lanes each
+    // issuing one compiled to a loop over the lanes that cost about 8 instructions per decode step.
     __device__ __forceinline__ void x_copy(int t, int seg, int w, int lane) {
-        if (lane == 0) mbar_arrive_expect_tx(&xbar[t], (uint32_t)kXBytes);
-        __syncwarp();
-        if (lane < (int)kHoles)
-            bulk_g2s(sm0 + xb + ((uint32_t)t * kHoles + (uint32_t)lane) * cst,
-                     tiles + ((size_t)seg * nwin + w) * kXBytes + (size_t)lane * 128, 128u, &xbar[t]);
+        const int8_t *src = tiles + ((size_t)seg * nwin + w) * kXBytes;
+        unsigned char *dst = sm0 + xb + (uint32_t)t * kHoles * cst;
+#pragma unroll
+        for (uint32_t i = 0; i < kXBytes / 512; i++) {
+            const uint32_t k = (uint32_t)lane + 32u * i;
+            cp_async_16(dst + (k >> 3) * cst + (k & 7u) * 16u, src + (size_t)k * 16);
+        }
+        cp_async_mbar_arrive_noinc(&xbar[t]);
         if (t) xcnt1++;
         else xcnt0++;
     }
+    // The window's copies (generic proxy) are visible to every lane once the barrier phase completes; the
+    // proxy fence orders them before the tensor core's reads of the tile (async proxy).
     __device__ __forceinline__ void x_wait(const Q8SLaunch &L, int t) {
         const uint32_t n = t ? xcnt1 : xcnt0;
         // on a timeout (flagged) wait once more, bounded, so that no copy is left in flight
         if (!mbar_wait_bounded(&xbar[t], (n - 1) & 1, L.status, L.spin_limit))
             mbar_wait_bounded(&xbar[t], (n - 1) & 1, nullptr, L.spin_limit);
+        fence_proxy_async_smem();
     }
     // wait until every MMA issued so far completed (the latest commit covers all earlier MMAs)
     __device__ __forceinline__ bool wait_mma(const Q8SLaunch &L) {
@@ -1028,10 +1036,13 @@ struct MmaCons {
                 }
             }
         }
-        fence_proxy_async_smem();  // these generic accesses come before later bulk copies into the tiles
+        fence_proxy_async_smem();  // these generic accesses come before the tensor core's later reads of the tiles
         __syncthreads();  // the x tiles are written again (tables, x) by the next item
     }
-    __device__ __forceinline__ void drain(const Q8SLaunch &L) { wait_mma(L); }
+    __device__ __forceinline__ void drain(const Q8SLaunch &L) {
+        wait_mma(L);
+        cp_async_wait_all();  // no x copy is left writing shared memory after the CTA exits
+    }
 };
 
 // four int8 weights (packed) -> four bf16 (exact: |w| <= 127 needs 7 significand bits), as two bf16x2
