@@ -1019,10 +1019,16 @@ struct MmaCons {
         tcgen05_fence_before();
         __syncthreads();
         const mv_q8_view &m = J.m;
+        const int W8 = min(W, 8);
         for (int t = threadIdx.x; t < 16 * 32; t += blockDim.x) {
             const int v = t >> 5, l = t & 31;
             int sum = 0;
-            for (int w = 0; w < W; w++)
+            // warps 0..7: tile 0 at hole 32 w (byte 8192 w + 128), core matrix v one 256-byte row further
+            const unsigned char *h = sm0 + 128u + (uint32_t)v * 256u + 4u * (uint32_t)l;
+#pragma unroll
+            for (int w = 0; w < 8; w++)
+                if (w < W8) sum += *reinterpret_cast<const int *>(h + (uint32_t)w * 2u * kHoles * 256u);
+            for (int w = 8; w < W; w++)
                 sum += *reinterpret_cast<const int *>(sm0 + tile_base(L, w) + (uint32_t)v * tile_stride(w) + 4 * l);
             const int row = stripe * 32 + l;
             if (row < m.rows && v < L.batch) {
@@ -1591,29 +1597,56 @@ __device__ __forceinline__ void build_table(const Q8SLaunch &L, const mv_q8_view
         return;
     }
     uint32_t k = o0;
-    if (kWide && cum < (uint32_t)qlo) {
-        // symbols that end at or before qlo: one load, shift and add each (measured: 0.8 % faster for
-        // the CUDA-core consumers, 0.6 % slower for the tensor-core one, which keeps the plain loop)
-        uint32_t f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
-        while (k < o1 && cum + f <= (uint32_t)qlo) {
-            cum += f;
-            k++;
-            f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+    if constexpr (kWide) {
+        if (cum < (uint32_t)qlo) {
+            // symbols that end at or before qlo: one load, shift and add each (measured: 0.8 % faster than
+            // the plain loop below; the four-at-a-time walk of the narrow layouts measured 1.5 % slower here)
+            uint32_t f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+            while (k < o1 && cum + f <= (uint32_t)qlo) {
+                cum += f;
+                k++;
+                f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+            }
         }
-    }
-    for (; k < o1 && cum < (uint32_t)qhi; k++) {
-        const uint32_t ent = tsm[k];
-        const uint32_t f = ent >> 8, sym = ent & 0xFF;
-        const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
-        if constexpr (kWide) {
+        for (; k < o1 && cum < (uint32_t)qhi; k++) {
+            const uint32_t ent = tsm[k];
+            const uint32_t f = ent >> 8, sym = ent & 0xFF;
+            const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
             for (uint32_t q = a; q < e; q++)
                 reinterpret_cast<uint2 *>(lut)[q * 32 + lane] = make_uint2(f | (sym << 16), q - cum);
-        } else {
+            cum += f;
+        }
+    } else {
+        if (cum < (uint32_t)qlo) {
+            // symbols that end at or before qlo, four at a time: the four loads are independent, so the walk
+            // waits for shared memory once per four symbols instead of once per symbol (the later warps of a
+            // CTA skip most of a row's list, and the CTA barrier after the build waits for them)
+            while (k + 4 <= o1) {
+                const uint32_t c4 = cum + ((uint32_t)tsm[k] >> 8) + ((uint32_t)tsm[k + 1] >> 8) +
+                                    ((uint32_t)tsm[k + 2] >> 8) + ((uint32_t)tsm[k + 3] >> 8);
+                if (c4 > (uint32_t)qlo) break;
+                cum = c4;
+                k += 4;
+            }
+            uint32_t f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+            while (k < o1 && cum + f <= (uint32_t)qlo) {
+                cum += f;
+                k++;
+                f = k < o1 ? (uint32_t)tsm[k] >> 8 : 0u;
+            }
+        }
+        // the next symbol's entry is loaded before this one's stores, off the walk's dependency chain
+        uint32_t ent = k < o1 ? (uint32_t)tsm[k] : 0u;
+        for (; k < o1 && cum < (uint32_t)qhi; k++) {
+            const uint32_t cur = ent;
+            ent = k + 1 < o1 ? (uint32_t)tsm[k + 1] : 0u;
+            const uint32_t f = cur >> 8, sym = cur & 0xFF;
+            const uint32_t a = max(cum, (uint32_t)qlo), e = min(cum + f, (uint32_t)qhi);
             // unrolled: measured 1 % faster for the tensor-core consumer (0.4 % slower for the wide table)
 #pragma unroll 4
             for (uint32_t q = a; q < e; q++) lut[q * kPitch + lane] = f | (sym << 16) | ((q - cum) << 24);
+            cum += f;
         }
-        cum += f;
     }
     if (cum < (uint32_t)qhi) {
         for (uint32_t q = max(cum, (uint32_t)qlo); q < (uint32_t)qhi; q++) {
