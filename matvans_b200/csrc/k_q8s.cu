@@ -810,7 +810,7 @@ struct MmaCons {
     static __device__ __forceinline__ uint32_t tile_stride(int w) { return w < 8 ? 256u : 128u; }
     uint32_t xt, d_tmem, st_addr, ld_addr, ncommit, xcur, xcnt0, xcnt1, xb, cst;
     uint64_t b_desc0;
-    uint64_t *mbar, *xbar;
+    uint32_t mbar, xbar;  // shared-memory addresses: the MMA barrier, the two x-window barriers (8 bytes apart)
     unsigned char *sm0;  // start of shared memory (table and holes)
     const int8_t *x;
     const int8_t *tiles;  // x laid out per (segment, window) by q8s_build_x_tiles, or null
@@ -826,13 +826,15 @@ struct MmaCons {
         xb = tile_base(L, warp);
         cst = tile_stride(warp);
         xt = smem_u32(sm0) + xb;  // tile 0, core matrix 0
-        mbar = reinterpret_cast<uint64_t *>(extra + xr_bytes(W)) + warp;
-        xbar = reinterpret_cast<uint64_t *>(extra + xr_bytes(W) + (size_t)W * 8) + 2 * warp;
+        uint64_t *mb = reinterpret_cast<uint64_t *>(extra + xr_bytes(W)) + warp;
+        uint64_t *xbp = reinterpret_cast<uint64_t *>(extra + xr_bytes(W) + (size_t)W * 8) + 2 * warp;
         if (lane == 0) {
-            mbar_init(mbar, 1);
-            mbar_init(&xbar[0], 32);  // x windows: one arrival per lane (x_copy)
-            mbar_init(&xbar[1], 32);
+            mbar_init(mb, 1);
+            mbar_init(&xbp[0], 32);  // x windows: one arrival per lane (x_copy)
+            mbar_init(&xbp[1], 32);
         }
+        mbar = smem_u32(mb);
+        xbar = smem_u32(xbp);
         fence_mbar_init();
         __syncwarp();
         // TMEM addresses: lane in bits [16,32), column in [0,16); a warp may touch only the 32 lanes of its
@@ -863,13 +865,13 @@ struct MmaCons {
     // issuing one compiled to a loop over the lanes that cost about 8 instructions per decode step.
     __device__ __forceinline__ void x_copy(int t, int seg, int w, int lane) {
         const int8_t *src = tiles + ((size_t)seg * nwin + w) * kXBytes;
-        unsigned char *dst = sm0 + xb + (uint32_t)t * kHoles * cst;
+        const uint32_t dst = xt + (uint32_t)t * kHoles * cst;
 #pragma unroll
         for (uint32_t i = 0; i < kXBytes / 512; i++) {
             const uint32_t k = (uint32_t)lane + 32u * i;
             cp_async_16(dst + (k >> 3) * cst + (k & 7u) * 16u, src + (size_t)k * 16);
         }
-        cp_async_mbar_arrive_noinc(&xbar[t]);
+        cp_async_mbar_arrive_noinc(xbar + 8u * (uint32_t)t);
         if (t) xcnt1++;
         else xcnt0++;
     }
@@ -878,8 +880,9 @@ struct MmaCons {
     __device__ __forceinline__ void x_wait(const Q8SLaunch &L, int t) {
         const uint32_t n = t ? xcnt1 : xcnt0;
         // on a timeout (flagged) wait once more, bounded, so that no copy is left in flight
-        if (!mbar_wait_bounded(&xbar[t], (n - 1) & 1, L.status, L.spin_limit))
-            mbar_wait_bounded(&xbar[t], (n - 1) & 1, nullptr, L.spin_limit);
+        const uint32_t bar = xbar + 8u * (uint32_t)t;
+        if (!mbar_wait_bounded(bar, (n - 1) & 1, L.status, L.spin_limit))
+            mbar_wait_bounded(bar, (n - 1) & 1, nullptr, L.spin_limit);
         fence_proxy_async_smem();
     }
     // wait until every MMA issued so far completed (the latest commit covers all earlier MMAs)

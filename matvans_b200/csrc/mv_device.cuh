@@ -44,25 +44,32 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+// The waits take the barrier as a shared-memory address (32-bit) or as a pointer into shared memory.
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(bar), "r"(parity)
         : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    return mbar_try_wait(smem_u32(bar), parity);
+}
 
 // Bounded wait; returns false (and raises MV_DEV_WAIT_TIMEOUT) on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t *status,
-                                                  uint32_t limit) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint32_t *status, uint32_t limit) {
     for (uint32_t it = 0; it < limit; it++)
         if (mbar_try_wait(bar, parity)) return true;
     if (status) atomicOr(status, MV_DEV_WAIT_TIMEOUT);
     return false;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t *status,
+                                                  uint32_t limit) {
+    return mbar_wait_bounded(smem_u32(bar), parity, status, limit);
 }
 
 // 4-byte asynchronous copy global -> shared (cp.async, no registers): src_bytes (0, 2 or 4) are read, the
@@ -75,14 +82,16 @@ __device__ __forceinline__ void cp_async_4(void *dst, const void *src, uint32_t 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// 16-byte asynchronous copy global -> shared, cached in L2 only; dst and src 16-byte aligned.
-__device__ __forceinline__ void cp_async_16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+// 16-byte asynchronous copy global -> shared (dst a shared-memory address), cached in L2 only; dst and src
+// 16-byte aligned.
+__device__ __forceinline__ void cp_async_16(uint32_t dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
-// Arrive on an mbarrier once every cp.async this thread issued so far has landed, without raising the
-// barrier's expected count: the barrier's arrival count must include one arrival per thread that calls this.
-__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t *bar) {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+// Arrive on an mbarrier (shared-memory address) once every cp.async this thread issued so far has landed,
+// without raising the barrier's expected count: the barrier's arrival count must include one arrival per
+// thread that calls this.
+__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint32_t bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ uint4 ldg_nc_u4(const uint4 *p) {

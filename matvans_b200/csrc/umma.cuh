@@ -135,10 +135,11 @@ __device__ __forceinline__ bool elect_one() {
 
 // Arrive once on `bar` when every tcgen05 operation issued so far by this
 // thread has completed.
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
 }
+__device__ __forceinline__ void umma_commit(uint64_t *bar) { umma_commit(smem_u32(bar)); }
 
 // Make this thread's generic-proxy shared-memory writes visible to the
 // tensor core (async proxy).
