@@ -233,7 +233,8 @@ mv_status mv_q8_matvec_tuned(const mv_q8_view *m, const int8_t *x_dev, int batch
  * is device scratch of mv_q8_x_tiles_bytes(&m) bytes, 16-byte aligned: with
  * 8..16 vectors on the tensor cores, mv_q8_stack_matvec first lays x out there
  * in the MMA operand layout, and each warp then brings its x windows in with
- * one asynchronous bulk copy instead of per-lane loads and stores. */
+ * asynchronous copies (four 16-byte cp.async per lane per window, completing
+ * on an mbarrier) instead of loads and stores through registers. */
 typedef struct mv_q8_job {
     mv_q8_view m;
     const int8_t *x;
