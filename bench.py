@@ -327,7 +327,7 @@ def chain_section(torch, ops, autotune, dev, mats, batches=(1, 16), reps=5, scal
 
 def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, reps=10):
     """The 224-matrix uneven stack, one persistent launch per step, B in {1,4,8,16}; the tensor-core
-    engine competes with dp4a at B >= 8.  Gate: bit-exact against the dense int8 kernel on the same x."""
+    engine competes with dp4a from 3 vectors on.  Gate: bit-exact against the dense int8 kernel on the same x."""
     t_build = time.perf_counter()
     mats = build_stack(torch, ops, dev, layers)
     t_build = time.perf_counter() - t_build
@@ -362,8 +362,8 @@ def stack_section(torch, ops, autotune, dev, batches=(1, 4, 8, 16), layers=32, r
         best, res = autotune.tune_stack(lambda t: ops.Q8Stack(Ms, batch=B, tuning=t, xs=xs, device=dev),
                                         candidates=cands, reps=reps, key=autotune.stack_key(Ms, B))
         row = {}
-        # tensor cores: engine 0; CUDA cores: engine 1 (0 below 8 vectors)
-        groups = {"tcgen05": (0,), "dp4a": (1,)} if B >= 8 else {"dp4a": (0,)}
+        # tensor cores: engine 0; CUDA cores: engine 1 (0 below the tensor cores' smallest batch)
+        groups = {"tcgen05": (0,), "dp4a": (1,)} if B >= ops.MMA_MIN_BATCH else {"dp4a": (0,)}
         for name, engs in groups.items():
             mine = {k: v for k, v in res.items() if int(k.split(",")[5]) in engs}
             if not mine:

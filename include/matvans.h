@@ -211,9 +211,11 @@ mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int3
  *   parts        work items per 32-row stripe (its segments split in `parts`
  *                ranges; default: whole stripes in stacks, enough parts to
  *                fill the GPU for a single matrix)
- *   engine       int8 product of 8..16 vectors: 0 = tensor cores
- *                (tcgen05.mma kind::i8, TMEM accumulators; ilp is then 1),
- *                1 = CUDA cores (dp4a).  Fewer vectors always use dp4a. */
+ *   engine       int8 product of 3..16 vectors: 0 = tensor cores
+ *                (tcgen05.mma kind::i8, TMEM accumulators, always 16
+ *                vectors wide with the missing ones zero; ilp is then 1),
+ *                1 = CUDA cores (dp4a).  One or two vectors always use
+ *                dp4a. */
 #define MV_ENGINE_AUTO 0
 #define MV_ENGINE_DP4A 1
 typedef struct mv_q8_tuning {
@@ -231,7 +233,7 @@ mv_status mv_q8_matvec_tuned(const mv_q8_view *m, const int8_t *x_dev, int batch
  * outputs y [batch][rows] (+ optional scaled output).  ngroups, atomic and
  * item0 are filled in by mv_q8_stack_plan.  x_tiles (optional, NULL for none)
  * is device scratch of mv_q8_x_tiles_bytes(&m) bytes, 16-byte aligned: with
- * 8..16 vectors on the tensor cores, mv_q8_stack_matvec first lays x out there
+ * 3..16 vectors on the tensor cores, mv_q8_stack_matvec first lays x out there
  * in the MMA operand layout, and each warp then brings its x windows in with
  * asynchronous copies (four 16-byte cp.async per lane per window, completing
  * on an mbarrier) instead of loads and stores through registers. */

@@ -31,9 +31,10 @@ SINGLE_CANDIDATES = CANDIDATES + [(w, ilp, d, 0, p, 0) for w in (4, 8) for ilp i
 
 
 def candidates_for(batch, base):
-    """Candidates at `batch` vectors: 8..16 vectors run on the tensor cores
-    (engine 0, where ilp is fixed at 1) or on the CUDA cores (engine 1)."""
-    if batch < 8:
+    """Candidates at `batch` vectors: from MMA_MIN_BATCH (3) vectors on they run
+    on the tensor cores (engine 0, where ilp is fixed at 1) or on the CUDA cores
+    (engine 1); fewer vectors always use the CUDA cores."""
+    if batch < _lib.MMA_MIN_BATCH:
         return list(base)
     mma = sorted({(w, 1, c[2], c[3], c[4], 0) for c in base for w in (4, 6, 8)})  # at most 8 warps
     return mma + [c[:5] + (1,) for c in base]

@@ -11,7 +11,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import Q8Job, Q8StackInfo, Q8Tuning, Q8View, check, lib
+from ._lib import MMA_MIN_BATCH, Q8Job, Q8StackInfo, Q8Tuning, Q8View, check, lib
 
 _STATUS_BITS = {1: "stream overrun", 2: "final coder state mismatch", 4: "wait timeout", 8: "bad table"}
 
@@ -299,9 +299,9 @@ class Q8Stack:
                     for M in self.matrices] if scales is not None else None
         n = len(self.matrices)
         jobs = (Q8Job * n)()
-        # 5..16 vectors (rounded up to 8 or 16) run on the tensor cores: x is laid out in tiles first
-        # (device scratch per matrix)
-        self._tiled = self.batch >= 5 and self.tuning.engine == 0
+        # 3..16 vectors run on the tensor cores (engine 0): x is laid out in tiles first (device scratch per
+        # matrix)
+        self._tiled = self.batch >= MMA_MIN_BATCH and self.tuning.engine == 0
         use_tiles = self._tiled
         self.x_tiles = []
         for i, M in enumerate(self.matrices):

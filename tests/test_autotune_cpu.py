@@ -11,15 +11,16 @@ from matvans_b200 import autotune
 def test_candidates_per_batch():
     base = autotune.SINGLE_CANDIDATES
     assert autotune.candidates_for(1, base) == list(base)
-    assert autotune.candidates_for(4, base) == list(base)
-    c16 = autotune.candidates_for(16, base)
-    mma = [c for c in c16 if c[5] == 0]
-    dp4a = [c for c in c16 if c[5] == 1]
-    assert mma and dp4a
-    assert all(c[1] == 1 for c in mma)                       # the tensor-core engine decodes with ilp 1
-    assert {c[0] for c in mma} == {4, 6, 8}                  # up to 8 warps per CTA there
-    assert sorted(c[:5] for c in dp4a) == sorted(c[:5] for c in base)  # every base candidate on the CUDA cores
-    assert len(set(c16)) == len(c16)
+    assert autotune.candidates_for(2, base) == list(base)   # one or two vectors: the CUDA cores only
+    for B in (3, 4, 8, 16):                                  # from 3 vectors on: both engines
+        cb = autotune.candidates_for(B, base)
+        mma = [c for c in cb if c[5] == 0]
+        dp4a = [c for c in cb if c[5] == 1]
+        assert mma and dp4a
+        assert all(c[1] == 1 for c in mma)                   # the tensor-core engine decodes with ilp 1
+        assert {c[0] for c in mma} == {4, 6, 8}              # up to 8 warps per CTA there
+        assert sorted(c[:5] for c in dp4a) == sorted(c[:5] for c in base)  # every base candidate on CUDA cores
+        assert len(set(cb)) == len(cb)
 
 
 def test_cache_round_trip_and_damaged_file(tmp_path, monkeypatch):

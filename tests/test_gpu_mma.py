@@ -1,5 +1,6 @@
 """Tensor-core (tcgen05.mma kind::i8) consumer of the persistent Q8 kernel:
-8..16 int8 vectors, exact int32 accumulation in tensor memory.  Every case is
+3..16 int8 vectors (multiplied 16 wide, the missing ones zero), exact int32
+accumulation in tensor memory.  Every case is
 compared bit for bit with the CPU oracle and with the CUDA-core dp4a engine
 on the same launch parameters."""
 import numpy as np
@@ -40,7 +41,7 @@ def _both_engines(M, W, x, s, tuning):
     assert np.array_equal(ys0.cpu().numpy(), sref)
 
 
-@pytest.mark.parametrize("B", [8, 9, 12, 15, 16])
+@pytest.mark.parametrize("B", [3, 4, 5, 8, 9, 12, 15, 16])
 @pytest.mark.parametrize("local", [True, False])
 def test_mma_batches(B, local):
     rng = np.random.default_rng(B + 100 * local)
@@ -118,7 +119,7 @@ def test_mma_stack(engine):
     shapes = [(512, 512), (1376, 512), (512, 1376), (96, 4096), (33, 208)]
     Ws = [gauss(rng, rng.uniform(2, 6), sh) for sh in shapes]
     Ms = [ops.Q8Matrix.encode(W, local=(i % 2 == 0)) for i, W in enumerate(Ws)]
-    for B in (8, 16):
+    for B in (3, 4, 8, 16):
         for tuning in ((4, 1, 1, 0, 0), (8, 1, 2, 0, 2)):
             xs = [torch.from_numpy(rng.integers(-127, 128, size=(B, M.cols)).astype(np.int8)).cuda() for M in Ms]
             S = ops.Q8Stack(Ms, batch=B, tuning=tuning + (engine,), xs=xs)
