@@ -41,6 +41,7 @@
 //             u01 + (f0 f1) t2, P = (f0 f1)(f2 f3), (hi:lo) = hi*P + t0 (one
 //             32x32->64 IMAD)
 #include <algorithm>
+#include <type_traits>
 #include <cstdio>
 
 #include <cuda_bf16.h>
@@ -949,11 +950,13 @@ struct MmaCons {
             load_window(xr, xrow, xok, colbase, 0, npieces);
         }
         SegStream S(sm, soff, rows_now[0], lane);
-        // pieces in pairs: piece p = 2 * pair (+1); a window holds 2 pairs
-        for (int p = 0; p < npieces; p += 2) {
+        // pieces in pairs: piece p = 2 * pair (+1); a window holds 2 pairs.  A pair of two full pieces (16
+        // quads) takes the body without the tail tests; the segment's last pair may be partial.
+        auto pair = [&](const int p, auto full) {
+            constexpr bool kFull = decltype(full)::value;
             uint32_t w[8];
             const int qc = 8 * p;
-            if (qc + 8 <= nq) {
+            if (kFull || qc + 8 <= nq) {
 #pragma unroll
                 for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut, kLut256>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
             } else {
@@ -986,10 +989,10 @@ struct MmaCons {
             }
             tcgen05_fence_after();
             tmem_st_32x32b_x8_nowait(st_addr, w);
-            const bool two = p + 1 < npieces;
+            const bool two = kFull || p + 1 < npieces;
             if (two) {
                 const int qc2 = qc + 8;
-                if (qc2 + 8 <= nq) {
+                if (kFull || qc2 + 8 <= nq) {
 #pragma unroll
                     for (int j = 0; j < 8; j++) w[j] = q8_step_t<kWideLut, kLut256>(S.lo, S.hi, S.koff, S.kend, sm, lut_l, L.lut_stride, lane, S.P);
                 } else {
@@ -1001,7 +1004,10 @@ struct MmaCons {
             }
             tmem_wait_st();
             issue(pw, two);
-        }
+        };
+        const int pfull = (nq >> 4) << 1;  // pieces covered by full pairs
+        for (int p = 0; p < pfull; p += 2) pair(p, std::true_type{});
+        if (pfull < npieces) pair(pfull, std::false_type{});
         if (!S.ok()) atomicOr(L.status, MV_DEV_FINAL_STATE);
     }
     __device__ __forceinline__ void finish_item(const Q8SLaunch &L, const Q8Job &J, int stripe, int warp, int lane,
