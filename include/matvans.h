@@ -218,6 +218,9 @@ mv_status mv_q8_matvec(const mv_q8_view *m, const int8_t *x_dev, int batch, int3
  *                dp4a. */
 #define MV_ENGINE_AUTO 0
 #define MV_ENGINE_DP4A 1
+/* Smallest integer batch that engine 0 (MV_ENGINE_AUTO) runs on the tensor
+ * cores. */
+#define MV_MMA_MIN_VECTORS 3
 typedef struct mv_q8_tuning {
     int32_t warps, ilp, depth, ctas_per_sm, parts, engine;
 } mv_q8_tuning;

@@ -16,8 +16,8 @@ MV_OK = 0
 STATUS_NAMES = {1: "MV_ERR_ARG", 2: "MV_ERR_SHAPE", 3: "MV_ERR_FORMAT", 4: "MV_ERR_IO", 5: "MV_ERR_CUDA",
                 6: "MV_ERR_DEVICE", 7: "MV_ERR_NOMEM", 8: "MV_ERR_UNSUPPORTED"}
 DEV_STREAM_OVERRUN, DEV_FINAL_STATE, DEV_WAIT_TIMEOUT, DEV_BAD_TABLE = 1, 2, 4, 8
-# integer batches of at least this many vectors run on the tensor cores with engine 0 (the library's
-# kMmaMinVectors); smaller ones always use dp4a
+# integer batches of at least this many vectors run on the tensor cores with engine 0
+# (MV_MMA_MIN_VECTORS in include/matvans.h); smaller ones always use dp4a
 MMA_MIN_BATCH = 3
 
 # every symbol include/matvans.h declares

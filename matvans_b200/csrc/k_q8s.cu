@@ -2005,7 +2005,7 @@ mv_status launch_q8s_c(const Q8SLaunch &L, const mv_q8_tuning &t, cudaStream_t s
 // (engine 0), which always multiplies 16 vectors, the missing ones zero: its cost hardly depends on the batch
 // (the 224-matrix stack: 3.86 ms at 8 vectors, 3.88 ms at 16), while the dp4a consumer's grows with it (4.25
 // ms at 4 vectors, 2.91 ms at 1).
-constexpr int kMmaMinVectors = 3;
+constexpr int kMmaMinVectors = MV_MMA_MIN_VECTORS;
 
 mv_status launch_q8s(const Q8SLaunch &L, int nv, const mv_q8_tuning &t, cudaStream_t st) {
     if (nv >= kMmaMinVectors && t.engine == MV_ENGINE_AUTO) return launch_q8s_c<MmaCons>(L, t, st);

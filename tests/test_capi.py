@@ -60,3 +60,10 @@ def test_stack_plan_reports_atomic_jobs():
     assert [by_cols[c].ngroups for c in (512, 64, 1024)] == [4, 1, 4]
     assert info.atomic_jobs == 2 and [by_cols[c].atomic for c in (512, 64, 1024)] == [1, 0, 1]
     assert info.nitems == 2 * 4 + 1 + 3 * 4
+
+
+def test_tensor_core_threshold_matches_the_header():
+    """The Python side's batch threshold for the tensor-core engine (ops, autotuner, bench) is the library's."""
+    src = open(os.path.join(ROOT, "include", "matvans.h")).read()
+    m = re.search(r"#define\s+MV_MMA_MIN_VECTORS\s+(\d+)", src)
+    assert m and int(m.group(1)) == _lib.MMA_MIN_BATCH
